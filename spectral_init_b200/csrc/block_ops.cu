@@ -1,0 +1,818 @@
+// Dense block kernels of the eigensolvers: tall-skinny Gram products,
+// block combinations, the fused LOBPCG update, column norms, the seeded
+// starting block, and the selection / sign / scaling steps of the pipeline
+// (src/selection.rs:11-29, src/scaling.rs:9-89).
+//
+// All reductions are deterministic: every CTA writes its partial sums, and
+// the last CTA to finish (atomic ticket) adds them in CTA order.
+#include <algorithm>
+#include <vector>
+
+#include "si_internal.h"
+
+namespace si {
+
+void GramWork::ensure(size_t partial_count, cudaStream_t s) {
+  if (partial.size() < partial_count) partial.alloc(partial_count, s);
+  if (counter.size() < 1) {
+    counter.alloc(1, s);
+    counter.zero();
+  }
+}
+
+namespace {
+
+constexpr int GT = 256;         // threads per Gram CTA
+constexpr int GTR = 32;         // rows per smem tile
+constexpr int GEPT = 17;        // entries per thread (covers a 64 x 64 full product)
+constexpr int GMAXE = GT * GEPT;
+constexpr int GMAXW = 8 * MAXM; // widest tile row (8 blocks of 16)
+
+template <class XT>
+struct GramParams {
+  const XT* blk[8];
+  int nblk, ns, m, ld, mode, ne, P, Q;
+  int64_t n;
+  double* partial;
+  double* out;
+  unsigned* counter;
+  const int* stop;
+};
+
+// entry e -> (tile column a, tile column b, out index, mirrored out index)
+__device__ inline void gram_entry(int mode, int P, int Q, int e, int& a, int& b, int& o1, int& o2) {
+  if (mode == GRAM_FULL) {
+    a = e / Q;
+    b = P + e % Q;
+    o1 = e;
+    o2 = -1;
+    return;
+  }
+  const int half = P * (P + 1) / 2;
+  const int which = e >= half ? 1 : 0;
+  int r = which ? e - half : e;
+  int i = 0;
+  while (r >= P - i) {
+    r -= P - i;
+    ++i;
+  }
+  const int j = i + r;
+  a = i;
+  b = which ? P + j : j;
+  o1 = which * P * P + i * P + j;
+  o2 = which * P * P + j * P + i;
+}
+
+template <class XT>
+__global__ void __launch_bounds__(GT) k_gram(GramParams<XT> p) {
+  if (p.stop != nullptr && *p.stop != 0) return;
+  __shared__ double tile[GTR][GMAXW + 1];
+  __shared__ bool last;
+  const int tid = threadIdx.x;
+  int ea[GEPT], eb[GEPT];
+  double acc[GEPT];
+  int cnt = 0;
+#pragma unroll
+  for (int q = 0; q < GEPT; ++q) {
+    const int e = tid + q * GT;
+    acc[q] = 0.0;
+    ea[q] = 0;
+    eb[q] = 0;
+    if (e < p.ne) {
+      int o1, o2;
+      gram_entry(p.mode, p.P, p.Q, e, ea[q], eb[q], o1, o2);
+      cnt = q + 1;
+    }
+  }
+  const int width = p.nblk * p.m;
+  const int64_t ntiles = (p.n + GTR - 1) / GTR;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t row0 = t * GTR;
+    for (int idx = tid; idx < GTR * width; idx += GT) {
+      const int b = idx / (GTR * p.m);
+      const int rem = idx % (GTR * p.m);
+      const int r = rem / p.m;
+      const int c = rem % p.m;
+      const int64_t row = row0 + r;
+      tile[r][b * p.m + c] = row < p.n ? static_cast<double>(p.blk[b][row * p.ld + c]) : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int r = 0; r < GTR; ++r) {
+#pragma unroll
+      for (int q = 0; q < GEPT; ++q)
+        if (q < cnt) acc[q] = fma(tile[r][ea[q]], tile[r][eb[q]], acc[q]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < GEPT; ++q)
+    if (q < cnt) p.partial[static_cast<int64_t>(blockIdx.x) * p.ne + tid + q * GT] = acc[q];
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(p.counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int e = tid; e < p.ne; e += GT) {
+    double s = 0.0;
+    for (int c = 0; c < static_cast<int>(gridDim.x); ++c) s += p.partial[static_cast<int64_t>(c) * p.ne + e];
+    int a, b, o1, o2;
+    gram_entry(p.mode, p.P, p.Q, e, a, b, o1, o2);
+    p.out[o1] = s;
+    if (o2 >= 0) p.out[o2] = s;
+  }
+  if (tid == 0) *p.counter = 0u;
+}
+
+// ---------------------------------------------------------------------------
+template <class XT>
+__global__ void k_combine(const XT* in0, const XT* in1, const XT* in2, const double* c0, const double* c1,
+                          const double* c2, int nin, XT* out, int m_in, int m_out, int cstride, int ld,
+                          int64_t n) {
+  extern __shared__ double sc_dyn[];
+  const int tot = m_in * m_out;
+  double* sc[3] = {sc_dyn, sc_dyn + tot, sc_dyn + 2 * tot};
+  for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+    const int src = (i / m_out) * cstride + i % m_out;
+    sc[0][i] = c0[src];
+    if (nin > 1) sc[1][i] = c1[src];
+    if (nin > 2) sc[2][i] = c2[src];
+  }
+  __syncthreads();
+  const XT* ins[3] = {in0, in1, in2};
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+    for (int j0 = 0; j0 < m_out; j0 += 4) {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int b = 0; b < nin; ++b) {
+        const XT* row = ins[b] + i * ld;
+        for (int c = 0; c < m_in; ++c) {
+          const double v = static_cast<double>(row[c]);
+#pragma unroll
+          for (int t = 0; t < 4; ++t)
+            if (j0 + t < m_out) acc[t] = fma(v, sc[b][c * m_out + j0 + t], acc[t]);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        if (j0 + t < m_out) out[i * ld + j0 + t] = static_cast<XT>(acc[t]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Column residual norms with deterministic reduction.
+template <class XT>
+__global__ void k_colnorms(const XT* a, const XT* b, const double* lam, int m, int ld, int64_t n, double* partial,
+                           unsigned* counter, double* out) {
+  __shared__ double red[8][MAXM];
+  __shared__ bool last;
+  double acc[MAXM];
+  double l[MAXM];
+#pragma unroll
+  for (int c = 0; c < MAXM; ++c) {
+    acc[c] = 0.0;
+    l[c] = (b != nullptr && c < m) ? lam[c] : 0.0;
+  }
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+#pragma unroll
+    for (int c = 0; c < MAXM; ++c) {
+      if (c < m) {
+        double d = static_cast<double>(a[i * ld + c]);
+        if (b != nullptr) d -= l[c] * static_cast<double>(b[i * ld + c]);
+        acc[c] = fma(d, d, acc[c]);
+      }
+    }
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int c = 0; c < MAXM; ++c) {
+    const double s = warp_sum(acc[c]);
+    if (lane == 0) red[warp][c] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < m) {
+    double s = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += red[w][threadIdx.x];
+    partial[static_cast<int64_t>(blockIdx.x) * MAXM + threadIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < m) {
+    double s = 0.0;
+    for (int c = 0; c < static_cast<int>(gridDim.x); ++c) s += partial[static_cast<int64_t>(c) * MAXM + threadIdx.x];
+    out[threadIdx.x] = sqrt(s);
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
+template <class XT>
+__global__ void k_fill_normal(XT* x, int64_t n, int m, int ld, uint64_t seed, uint64_t stream) {
+  const int64_t total = n * m;
+  const int64_t pairs = (total + 1) / 2;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < pairs; q += stride) {
+    double z0, z1;
+    philox_normal2(seed, stream, static_cast<uint64_t>(q), z0, z1);
+    const int64_t e0 = 2 * q, e1 = 2 * q + 1;
+    x[(e0 / m) * ld + e0 % m] = static_cast<XT>(z0);
+    if (e1 < total) x[(e1 / m) * ld + e1 % m] = static_cast<XT>(z1);
+  }
+}
+
+__global__ void k_sumsq(const double* v, int64_t n, double* partial, unsigned* counter, double* out) {
+  __shared__ double red[32];
+  __shared__ bool last;
+  double acc = 0.0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
+    acc = fma(v[i], v[i], acc);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += red[w];
+    partial[blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int c = 0; c < static_cast<int>(gridDim.x); ++c) s += partial[c];
+    *out = s;
+    *counter = 0u;
+  }
+}
+
+template <class XT>
+__global__ void k_set_col0(XT* x, int ld, int64_t n, const double* v, const double* sumsq) {
+  const double s = *sumsq;
+  if (!(s > 0.0)) return;
+  const double nrm = sqrt(s);
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
+    x[i * ld] = static_cast<XT>(v[i] / nrm);
+}
+
+template <class XT>
+__global__ void k_scale_cols(XT* x, int64_t n, int m, int ld, const double* s) {
+  const int64_t total = n * m;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total; e += stride) {
+    const int64_t i = e / m;
+    const int c = static_cast<int>(e % m);
+    x[i * ld + c] = static_cast<XT>(static_cast<double>(x[i * ld + c]) * s[c]);
+  }
+}
+
+struct ColList {
+  int c[SMAX];
+  int k;
+};
+
+template <class XI, class XO>
+__global__ void k_gather_cols(const XI* in, int ld_in, XO* out, int ld_out, int64_t n, ColList cols) {
+  const int64_t total = n * cols.k;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total; e += stride) {
+    const int64_t i = e / cols.k;
+    const int j = static_cast<int>(e % cols.k);
+    out[i * ld_out + j] = static_cast<XO>(in[i * ld_in + cols.c[j]]);
+  }
+}
+
+// per column: (max |x|, first index) ; deterministic
+__global__ void k_argmax_abs(const double* x, int64_t n, int k, int ld, double* pval, long long* pidx,
+                             unsigned* counter, double* sign_out) {
+  __shared__ double sv[256];
+  __shared__ long long si_[256];
+  __shared__ bool last;
+  for (int c = 0; c < k; ++c) {
+    double best = -1.0;
+    long long bi = -1;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+      const double a = fabs(x[i * ld + c]);
+      if (a > best) {
+        best = a;
+        bi = i;
+      }
+    }
+    sv[threadIdx.x] = best;
+    si_[threadIdx.x] = bi;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) {
+        const double a2 = sv[threadIdx.x + o];
+        const long long i2 = si_[threadIdx.x + o];
+        const double a1 = sv[threadIdx.x];
+        const long long i1 = si_[threadIdx.x];
+        if (i2 >= 0 && (a2 > a1 || (a2 == a1 && (i1 < 0 || i2 < i1)))) {
+          sv[threadIdx.x] = a2;
+          si_[threadIdx.x] = i2;
+        }
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      pval[static_cast<int64_t>(blockIdx.x) * SMAX + c] = sv[0];
+      pidx[static_cast<int64_t>(blockIdx.x) * SMAX + c] = si_[0];
+    }
+    __syncthreads();
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < k) {
+    const int c = threadIdx.x;
+    double best = -1.0;
+    long long bi = -1;
+    for (int b = 0; b < static_cast<int>(gridDim.x); ++b) {
+      const double a = pval[static_cast<int64_t>(b) * SMAX + c];
+      const long long i = pidx[static_cast<int64_t>(b) * SMAX + c];
+      if (i >= 0 && (a > best || (a == best && (bi < 0 || i < bi)))) {
+        best = a;
+        bi = i;
+      }
+    }
+    // Rust f64::signum: -1 for negative values and -0.0
+    sign_out[c] = (bi >= 0 && signbit(x[bi * ld + c])) ? -1.0 : 1.0;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
+__global__ void k_apply_signs(double* x, int64_t n, int k, int ld, const double* sign) {
+  const int64_t total = n * k;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total; e += stride) {
+    const int64_t i = e / k;
+    const int c = static_cast<int>(e % k);
+    if (sign[c] < 0.0) x[i * ld + c] = -x[i * ld + c];
+  }
+}
+
+__global__ void k_maxabs(const double* x, int64_t n, int k, int ld, double* partial, unsigned* counter,
+                         double* out) {
+  __shared__ double red[32];
+  __shared__ bool last;
+  double m = 0.0;
+  const int64_t total = n * k;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total; e += stride) {
+    const double a = fabs(x[(e / k) * ld + e % k]);
+    m = a > m ? a : m;  // NaN is ignored like f64::max
+  }
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s = fmax(s, red[w]);
+    partial[blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int c = 0; c < static_cast<int>(gridDim.x); ++c) s = fmax(s, partial[c]);
+    *out = s;
+    *counter = 0u;
+  }
+}
+
+__global__ void k_scale_noise(const double* x, int64_t n, int k, int ld, double expansion, uint64_t seed,
+                              float* out, int add_noise) {
+  const int64_t total = n * k;
+  const int64_t pairs = (total + 1) / 2;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < pairs; q += stride) {
+    double z[2] = {0.0, 0.0};
+    if (add_noise) philox_normal2(seed, 0x5ca1eull, static_cast<uint64_t>(q), z[0], z[1]);
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int64_t e = 2 * q + t;
+      if (e >= total) break;
+      const float s = static_cast<float>(x[(e / k) * ld + e % k] * expansion);
+      out[e] = add_noise ? __fadd_rn(s, __fmul_rn(static_cast<float>(z[t]), 1.0e-4f)) : s;
+    }
+  }
+}
+
+__global__ void k_copy_strided(const double* in, int ld_in, double* out, int ld_out, int64_t n, int k) {
+  const int64_t total = n * k;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total; e += stride)
+    out[(e / k) * ld_out + e % k] = in[(e / k) * ld_in + e % k];
+}
+
+// ---------------------------------------------------------------------------
+// LOBPCG update (one thread per row):
+//   P' = R Cr + P Cp,  AP' = AR Cr + AP Cp,  X' = X Cx + P',  AX' = AX Cx + AP',
+//   R' = AX' - X' diag(lam').  init mode: X' = X Cx, AX' = AX Cx, R' as above.
+// When the small step flagged the current X as the best iterate, the row of X
+// is first copied to Xbest.  Rows are updated in place.
+template <class XT, int LD>
+__global__ void __launch_bounds__(256) k_lobpcg_update(LobpcgBlocks<XT> b, const LobpcgCtrl* __restrict__ ctrl,
+                                                       int64_t n, int init_mode) {
+  __shared__ double sCx[MAXM * MAXM], sCr[MAXM * MAXM], sCp[MAXM * MAXM], sLam[MAXM];
+  __shared__ int sF[4];
+  if (threadIdx.x == 0) {
+    sF[0] = ctrl->done;
+    sF[1] = ctrl->copy_best;
+    sF[2] = ctrl->has_p;
+    sF[3] = ctrl->m;
+  }
+  __syncthreads();
+  const int done = sF[0], copy_best = sF[1], use_p = sF[2], m = sF[3];
+  if (done && !copy_best) return;
+  for (int i = threadIdx.x; i < m * m; i += blockDim.x) {
+    const int r = i / m, c = i % m;
+    sCx[r * MAXM + c] = ctrl->Cx[r * MAXM + c];
+    sCr[r * MAXM + c] = ctrl->Cr[r * MAXM + c];
+    sCp[r * MAXM + c] = ctrl->Cp[r * MAXM + c];
+  }
+  if (threadIdx.x < MAXM) sLam[threadIdx.x] = threadIdx.x < m ? ctrl->lam[threadIdx.x] : 0.0;
+  __syncthreads();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+    const int64_t o = i * LD;
+    double x[LD];
+#pragma unroll
+    for (int c = 0; c < LD; ++c) x[c] = static_cast<double>(b.X[o + c]);
+    if (copy_best) {
+#pragma unroll
+      for (int c = 0; c < LD; ++c) b.Xbest[o + c] = static_cast<XT>(x[c]);
+    }
+    if (done) continue;
+    double ax[LD];
+#pragma unroll
+    for (int c = 0; c < LD; ++c) ax[c] = static_cast<double>(b.AX[o + c]);
+    double xn[LD], axn[LD], pn[LD], apn[LD];
+#pragma unroll
+    for (int c = 0; c < LD; ++c) {
+      xn[c] = 0.0;
+      axn[c] = 0.0;
+      pn[c] = 0.0;
+      apn[c] = 0.0;
+    }
+    if (!init_mode) {
+      double r[LD], ar[LD];
+#pragma unroll
+      for (int c = 0; c < LD; ++c) {
+        r[c] = static_cast<double>(b.R[o + c]);
+        ar[c] = static_cast<double>(b.AR[o + c]);
+      }
+#pragma unroll
+      for (int c = 0; c < LD; ++c) {
+        if (c < m) {
+#pragma unroll
+          for (int j = 0; j < LD; ++j) {
+            if (j < m) {
+              pn[j] = fma(r[c], sCr[c * MAXM + j], pn[j]);
+              apn[j] = fma(ar[c], sCr[c * MAXM + j], apn[j]);
+            }
+          }
+        }
+      }
+      if (use_p) {
+        double p[LD], ap[LD];
+#pragma unroll
+        for (int c = 0; c < LD; ++c) {
+          p[c] = static_cast<double>(b.P[o + c]);
+          ap[c] = static_cast<double>(b.AP[o + c]);
+        }
+#pragma unroll
+        for (int c = 0; c < LD; ++c) {
+          if (c < m) {
+#pragma unroll
+            for (int j = 0; j < LD; ++j) {
+              if (j < m) {
+                pn[j] = fma(p[c], sCp[c * MAXM + j], pn[j]);
+                apn[j] = fma(ap[c], sCp[c * MAXM + j], apn[j]);
+              }
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < LD; ++c) {
+      if (c < m) {
+#pragma unroll
+        for (int j = 0; j < LD; ++j) {
+          if (j < m) {
+            xn[j] = fma(x[c], sCx[c * MAXM + j], xn[j]);
+            axn[j] = fma(ax[c], sCx[c * MAXM + j], axn[j]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < LD; ++j) {
+      xn[j] += pn[j];
+      axn[j] += apn[j];
+      b.X[o + j] = static_cast<XT>(xn[j]);
+      b.AX[o + j] = static_cast<XT>(axn[j]);
+      // residual from the stored (rounded) values so R matches AX - X lam of the block
+      const double xr = static_cast<double>(static_cast<XT>(xn[j]));
+      const double axr = static_cast<double>(static_cast<XT>(axn[j]));
+      b.R[o + j] = static_cast<XT>(j < m ? axr - sLam[j] * xr : 0.0);
+      if (!init_mode) {
+        b.P[o + j] = static_cast<XT>(pn[j]);
+        b.AP[o + j] = static_cast<XT>(apn[j]);
+      }
+    }
+  }
+}
+
+// Generic update for any ld (column loop, reads straight from global).
+template <class XT>
+__global__ void __launch_bounds__(256) k_lobpcg_update_generic(LobpcgBlocks<XT> b, const LobpcgCtrl* __restrict__ ctrl,
+                                                               int64_t n, int ld, int init_mode) {
+  __shared__ double sCx[MAXM * MAXM], sCr[MAXM * MAXM], sCp[MAXM * MAXM], sLam[MAXM];
+  __shared__ int sF[4];
+  if (threadIdx.x == 0) {
+    sF[0] = ctrl->done;
+    sF[1] = ctrl->copy_best;
+    sF[2] = ctrl->has_p;
+    sF[3] = ctrl->m;
+  }
+  __syncthreads();
+  const int done = sF[0], copy_best = sF[1], use_p = sF[2], m = sF[3];
+  if (done && !copy_best) return;
+  for (int i = threadIdx.x; i < MAXM * MAXM; i += blockDim.x) {
+    sCx[i] = ctrl->Cx[i];
+    sCr[i] = ctrl->Cr[i];
+    sCp[i] = ctrl->Cp[i];
+  }
+  if (threadIdx.x < MAXM) sLam[threadIdx.x] = threadIdx.x < m ? ctrl->lam[threadIdx.x] : 0.0;
+  __syncthreads();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+    const int64_t o = i * ld;
+    if (copy_best)
+      for (int c = 0; c < ld; ++c) b.Xbest[o + c] = b.X[o + c];
+    if (done) continue;
+    double xn[MAXM], axn[MAXM], pn[MAXM], apn[MAXM];
+#pragma unroll
+    for (int j = 0; j < MAXM; ++j) {
+      xn[j] = 0.0;
+      axn[j] = 0.0;
+      pn[j] = 0.0;
+      apn[j] = 0.0;
+    }
+    for (int c = 0; c < m; ++c) {
+      const double xv = static_cast<double>(b.X[o + c]);
+      const double axv = static_cast<double>(b.AX[o + c]);
+      double rv = 0.0, arv = 0.0, pv = 0.0, apv = 0.0;
+      if (!init_mode) {
+        rv = static_cast<double>(b.R[o + c]);
+        arv = static_cast<double>(b.AR[o + c]);
+        if (use_p) {
+          pv = static_cast<double>(b.P[o + c]);
+          apv = static_cast<double>(b.AP[o + c]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < MAXM; ++j) {
+        if (j < m) {
+          xn[j] = fma(xv, sCx[c * MAXM + j], xn[j]);
+          axn[j] = fma(axv, sCx[c * MAXM + j], axn[j]);
+          if (!init_mode) {
+            pn[j] = fma(rv, sCr[c * MAXM + j], pn[j]);
+            apn[j] = fma(arv, sCr[c * MAXM + j], apn[j]);
+            if (use_p) {
+              pn[j] = fma(pv, sCp[c * MAXM + j], pn[j]);
+              apn[j] = fma(apv, sCp[c * MAXM + j], apn[j]);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < MAXM; ++j) {
+      if (j < m) {
+        xn[j] += pn[j];
+        axn[j] += apn[j];
+        const XT xs = static_cast<XT>(xn[j]);
+        const XT axs = static_cast<XT>(axn[j]);
+        b.X[o + j] = xs;
+        b.AX[o + j] = axs;
+        b.R[o + j] = static_cast<XT>(static_cast<double>(axs) - sLam[j] * static_cast<double>(xs));
+        if (!init_mode) {
+          b.P[o + j] = static_cast<XT>(pn[j]);
+          b.AP[o + j] = static_cast<XT>(apn[j]);
+        }
+      }
+    }
+  }
+}
+
+int grid_rows(const Exec& ex, int64_t items, int threads = 256, int per_sm = 8) {
+  const int64_t need = (items + threads - 1) / threads;
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(ex.sms) * per_sm)));
+}
+
+}  // namespace
+
+template <class XT>
+void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, int ns, int nblk, int m, int ld,
+              int64_t n, double* out, const int* stop) {
+  SI_REQUIRE(nblk <= 8 && m <= MAXM && nblk * m <= GMAXW, SI_INVALID_ARGUMENT, "gram: too many columns");
+  GramParams<XT> p{};
+  for (int b = 0; b < nblk; ++b) p.blk[b] = blk[b];
+  p.nblk = nblk;
+  p.ns = ns;
+  p.m = m;
+  p.ld = ld;
+  p.n = n;
+  p.mode = mode;
+  p.P = ns * m;
+  if (mode == GRAM_SYM2) {
+    SI_REQUIRE(nblk == 2 * ns, SI_INVALID_ARGUMENT, "gram SYM2 needs 2*ns blocks");
+    p.Q = p.P;
+    p.ne = p.P * (p.P + 1);
+  } else {
+    p.Q = (nblk - ns) * m;
+    p.ne = p.P * p.Q;
+  }
+  SI_REQUIRE(p.ne <= GMAXE, SI_INVALID_ARGUMENT, "gram: too many entries");
+  const int64_t ntiles = (n + GTR - 1) / GTR;
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ex.sms) * 2)));
+  w.ensure(static_cast<size_t>(grid) * GMAXE, ex.stream);
+  p.partial = w.partial.get();
+  p.counter = w.counter.get();
+  p.out = out;
+  p.stop = stop;
+  k_gram<XT><<<grid, GT, 0, ex.stream>>>(p);
+  SI_LAUNCH_CHECK();
+}
+
+template <class XT>
+void combine_dev(const Exec& ex, const XT* const* in, const double* const* coef, int nin, XT* out, int m_in,
+                 int m_out, int cstride, int ld, int64_t n) {
+  SI_REQUIRE(nin >= 1 && nin <= 3 && m_in <= SMAX && m_out <= SMAX, SI_INVALID_ARGUMENT, "combine: bad sizes");
+  if (n == 0) return;
+  const size_t smem = sizeof(double) * nin * m_in * m_out;
+  SI_REQUIRE(smem <= 160 * 1024, SI_INVALID_ARGUMENT, "combine: coefficients too large");
+  if (smem > 48 * 1024)
+    SI_CUDA(cudaFuncSetAttribute(k_combine<XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  k_combine<XT><<<grid_rows(ex, n), 256, smem, ex.stream>>>(in[0], nin > 1 ? in[1] : nullptr,
+                                                          nin > 2 ? in[2] : nullptr, coef[0],
+                                                          nin > 1 ? coef[1] : nullptr, nin > 2 ? coef[2] : nullptr,
+                                                          nin, out, m_in, m_out, cstride, ld, n);
+  SI_LAUNCH_CHECK();
+}
+
+template <class XT>
+void column_residual_norms_dev(const Exec& ex, GramWork& w, const XT* a, const XT* b, const double* lam_dev, int m,
+                               int ld, int64_t n, double* out_dev) {
+  SI_REQUIRE(m <= MAXM, SI_INVALID_ARGUMENT, "colnorms: m too large");
+  const int grid = grid_rows(ex, std::max<int64_t>(n, 1), 256, 2);
+  w.ensure(static_cast<size_t>(grid) * MAXM, ex.stream);
+  k_colnorms<XT><<<grid, 256, 0, ex.stream>>>(a, b, lam_dev, m, ld, n, w.partial.get(), w.counter.get(), out_dev);
+  SI_LAUNCH_CHECK();
+}
+
+template <class XT>
+void fill_normal_dev(const Exec& ex, XT* x, int64_t n, int m, int ld, uint64_t seed, uint64_t stream) {
+  SI_CUDA(cudaMemsetAsync(x, 0, sizeof(XT) * n * ld, ex.stream));
+  if (n * m == 0) return;
+  k_fill_normal<XT><<<grid_rows(ex, (n * m + 1) / 2), 256, 0, ex.stream>>>(x, n, m, ld, seed, stream);
+  SI_LAUNCH_CHECK();
+}
+
+template <class XT>
+void set_column_normalized_dev(const Exec& ex, GramWork& w, XT* x, int ld, int64_t n, const double* v) {
+  if (n == 0) return;
+  const int grid = grid_rows(ex, n, 256, 2);
+  w.ensure(static_cast<size_t>(grid) + 1, ex.stream);
+  DevBuf<double> s(1, ex.stream);
+  k_sumsq<<<grid, 256, 0, ex.stream>>>(v, n, w.partial.get(), w.counter.get(), s.get());
+  SI_LAUNCH_CHECK();
+  k_set_col0<XT><<<grid_rows(ex, n), 256, 0, ex.stream>>>(x, ld, n, v, s.get());
+  SI_LAUNCH_CHECK();
+}
+
+template <class XT>
+void scale_columns_dev(const Exec& ex, XT* x, int64_t n, int m, int ld, const double* s) {
+  if (n * m == 0) return;
+  k_scale_cols<XT><<<grid_rows(ex, n * m), 256, 0, ex.stream>>>(x, n, m, ld, s);
+  SI_LAUNCH_CHECK();
+}
+
+template <class XI, class XO>
+void gather_columns_dev(const Exec& ex, const XI* in, int ld_in, XO* out, int ld_out, int64_t n,
+                        const std::vector<int>& cols) {
+  SI_REQUIRE(cols.size() <= static_cast<size_t>(SMAX), SI_INVALID_ARGUMENT, "gather: too many columns");
+  ColList cl{};
+  cl.k = static_cast<int>(cols.size());
+  for (size_t j = 0; j < cols.size(); ++j) cl.c[j] = cols[j];
+  if (n * cl.k == 0) return;
+  k_gather_cols<XI, XO><<<grid_rows(ex, n * cl.k), 256, 0, ex.stream>>>(in, ld_in, out, ld_out, n, cl);
+  SI_LAUNCH_CHECK();
+}
+
+void normalize_signs_dev(const Exec& ex, GramWork& w, double* x, int64_t n, int k, int ld) {
+  SI_REQUIRE(k <= SMAX, SI_INVALID_ARGUMENT, "normalize_signs: too many columns");
+  if (n == 0 || k == 0) return;
+  const int grid = grid_rows(ex, n, 256, 2);
+  DevBuf<double> pval(static_cast<size_t>(grid) * SMAX, ex.stream), sign(SMAX, ex.stream);
+  DevBuf<long long> pidx(static_cast<size_t>(grid) * SMAX, ex.stream);
+  w.ensure(1, ex.stream);
+  k_argmax_abs<<<grid, 256, 0, ex.stream>>>(x, n, k, ld, pval.get(), pidx.get(), w.counter.get(), sign.get());
+  SI_LAUNCH_CHECK();
+  k_apply_signs<<<grid_rows(ex, n * k), 256, 0, ex.stream>>>(x, n, k, ld, sign.get());
+  SI_LAUNCH_CHECK();
+}
+
+double max_abs_dev(const Exec& ex, GramWork& w, const double* x, int64_t n, int k, int ld) {
+  if (n * k == 0) return 0.0;
+  const int grid = grid_rows(ex, n * k, 256, 2);
+  w.ensure(static_cast<size_t>(grid), ex.stream);
+  DevBuf<double> out(1, ex.stream);
+  k_maxabs<<<grid, 256, 0, ex.stream>>>(x, n, k, ld, w.partial.get(), w.counter.get(), out.get());
+  SI_LAUNCH_CHECK();
+  double h = 0.0;
+  SI_CUDA(cudaMemcpyAsync(&h, out.get(), sizeof(double), cudaMemcpyDeviceToHost, ex.stream));
+  SI_CUDA(cudaStreamSynchronize(ex.stream));
+  return h;
+}
+
+void scale_noise_dev(const Exec& ex, const double* x, int64_t n, int k, int ld, double expansion, uint64_t seed,
+                     float* out, bool add_noise) {
+  if (n * k == 0) return;
+  k_scale_noise<<<grid_rows(ex, (n * k + 1) / 2), 256, 0, ex.stream>>>(x, n, k, ld, expansion, seed, out,
+                                                                        add_noise ? 1 : 0);
+  SI_LAUNCH_CHECK();
+}
+
+void copy_strided_dev(const Exec& ex, const double* in, int ld_in, double* out, int ld_out, int64_t n, int k) {
+  if (n * k == 0) return;
+  k_copy_strided<<<grid_rows(ex, n * k), 256, 0, ex.stream>>>(in, ld_in, out, ld_out, n, k);
+  SI_LAUNCH_CHECK();
+}
+
+template <class XT>
+void lobpcg_update_dev(const Exec& ex, const LobpcgBlocks<XT>& b, const LobpcgCtrl* ctrl, int ld, int64_t n,
+                       int init_mode) {
+  if (n == 0) return;
+  const int grid = grid_rows(ex, n);
+  if (ld == 4)
+    k_lobpcg_update<XT, 4><<<grid, 256, 0, ex.stream>>>(b, ctrl, n, init_mode);
+  else if (ld == 8)
+    k_lobpcg_update<XT, 8><<<grid, 256, 0, ex.stream>>>(b, ctrl, n, init_mode);
+  else
+    k_lobpcg_update_generic<XT><<<grid, 256, 0, ex.stream>>>(b, ctrl, n, ld, init_mode);
+  SI_LAUNCH_CHECK();
+}
+
+// explicit instantiations
+template void gram_dev<double>(const Exec&, GramWork&, GramMode, const double* const*, int, int, int, int, int64_t,
+                               double*, const int*);
+template void gram_dev<float>(const Exec&, GramWork&, GramMode, const float* const*, int, int, int, int, int64_t,
+                              double*, const int*);
+template void combine_dev<double>(const Exec&, const double* const*, const double* const*, int, double*, int, int,
+                                  int, int, int64_t);
+template void combine_dev<float>(const Exec&, const float* const*, const double* const*, int, float*, int, int,
+                                 int, int, int64_t);
+template void column_residual_norms_dev<double>(const Exec&, GramWork&, const double*, const double*,
+                                                const double*, int, int, int64_t, double*);
+template void column_residual_norms_dev<float>(const Exec&, GramWork&, const float*, const float*, const double*,
+                                               int, int, int64_t, double*);
+template void fill_normal_dev<double>(const Exec&, double*, int64_t, int, int, uint64_t, uint64_t);
+template void fill_normal_dev<float>(const Exec&, float*, int64_t, int, int, uint64_t, uint64_t);
+template void set_column_normalized_dev<double>(const Exec&, GramWork&, double*, int, int64_t, const double*);
+template void set_column_normalized_dev<float>(const Exec&, GramWork&, float*, int, int64_t, const double*);
+template void scale_columns_dev<double>(const Exec&, double*, int64_t, int, int, const double*);
+template void scale_columns_dev<float>(const Exec&, float*, int64_t, int, int, const double*);
+template void gather_columns_dev<double, double>(const Exec&, const double*, int, double*, int, int64_t,
+                                                 const std::vector<int>&);
+template void gather_columns_dev<float, double>(const Exec&, const float*, int, double*, int, int64_t,
+                                                const std::vector<int>&);
+template void gather_columns_dev<double, float>(const Exec&, const double*, int, float*, int, int64_t,
+                                                const std::vector<int>&);
+template void lobpcg_update_dev<double>(const Exec&, const LobpcgBlocks<double>&, const LobpcgCtrl*, int, int64_t,
+                                        int);
+template void lobpcg_update_dev<float>(const Exec&, const LobpcgBlocks<float>&, const LobpcgCtrl*, int, int64_t,
+                                       int);
+
+}  // namespace si

@@ -1,0 +1,530 @@
+// Small dense linear algebra in one CTA (matrices in shared memory):
+// Cholesky, triangular solves and a parallel cyclic Jacobi eigensolver, and
+// on top of them the per-iteration "small step" of block LOBPCG.
+//
+// LOBPCG small step (restatement of one iteration of the linfa-linalg 0.2
+// LOBPCG loop that src/solvers/lobpcg.rs:327-358 calls; algorithm of Knyazev,
+// SIAM J. Sci. Comput. 23(2), 2001):
+//   1. residual norms of the current block from diag(R^T R) of the Gram,
+//      best-iterate tracking (smallest sum of wanted residual norms), soft
+//      locking (a wanted column stays locked once its norm <= tol), and the
+//      convergence / iteration-cap decision;
+//   2. Rayleigh-Ritz on span{X, R_active, P_active} as the generalised
+//      problem (S^T A S) y = theta (S^T S) y, made well-scaled by the diagonal
+//      of S^T S and reduced with a Cholesky factor; when the factor fails
+//      with P present the step is retried on span{X, R_active} (the same
+//      fallback as the reference iteration);
+//   3. the coefficients Cx, Cr, Cp of the new X and P for the block update.
+// The Gram matrices come from the fused device pass over the blocks, so the
+// residuals never need an explicit orthogonalisation pass.
+#include <cfloat>
+
+#include "si_internal.h"
+
+namespace si {
+namespace {
+
+constexpr int ST = 128;  // threads of the small-step CTA
+
+struct SmallSmem {
+  double* A;
+  double* B;
+  double* V;
+  double* Z;
+  int ld;
+};
+
+__device__ void cta_identity(double* V, int s, int ld) {
+  for (int i = threadIdx.x; i < s * s; i += blockDim.x) V[(i / s) * ld + i % s] = (i / s == i % s) ? 1.0 : 0.0;
+}
+
+// In-place lower Cholesky; returns false if a pivot is <= tol.
+__device__ bool cta_cholesky(double* B, int s, int ld, double tol, int* sflag) {
+  for (int j = 0; j < s; ++j) {
+    if (threadIdx.x == 0) {
+      const double d = B[j * ld + j];
+      if (!(d > tol)) {
+        *sflag = 1;
+      } else {
+        B[j * ld + j] = sqrt(d);
+        *sflag = 0;
+      }
+    }
+    __syncthreads();
+    if (*sflag) return false;
+    const double piv = B[j * ld + j];
+    for (int i = j + 1 + threadIdx.x; i < s; i += blockDim.x) B[i * ld + j] /= piv;
+    __syncthreads();
+    const int w = s - j - 1;
+    for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
+      const int i = j + 1 + t / w, k = j + 1 + t % w;
+      if (k <= i) B[i * ld + k] -= B[i * ld + j] * B[k * ld + j];
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
+// M <- L^-1 M   (M: s x ncol), one thread per column.
+__device__ void cta_trsm_left_lower(const double* L, double* M, int s, int ncol, int ld) {
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+    for (int i = 0; i < s; ++i) {
+      double v = M[i * ld + c];
+      for (int k = 0; k < i; ++k) v -= L[i * ld + k] * M[k * ld + c];
+      M[i * ld + c] = v / L[i * ld + i];
+    }
+  }
+  __syncthreads();
+}
+
+// M <- M L^-T   (M: nrow x s), one thread per row.
+__device__ void cta_trsm_right_lowerT(const double* L, double* M, int s, int nrow, int ld) {
+  for (int r = threadIdx.x; r < nrow; r += blockDim.x) {
+    for (int j = 0; j < s; ++j) {
+      double v = M[r * ld + j];
+      for (int k = 0; k < j; ++k) v -= M[r * ld + k] * L[j * ld + k];
+      M[r * ld + j] = v / L[j * ld + j];
+    }
+  }
+  __syncthreads();
+}
+
+// M <- L^-T M   (M: s x ncol), one thread per column (back substitution).
+__device__ void cta_trsm_left_lowerT(const double* L, double* M, int s, int ncol, int ld) {
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+    for (int i = s - 1; i >= 0; --i) {
+      double v = M[i * ld + c];
+      for (int k = i + 1; k < s; ++k) v -= L[k * ld + i] * M[k * ld + c];
+      M[i * ld + c] = v / L[i * ld + i];
+    }
+  }
+  __syncthreads();
+}
+
+__device__ double cta_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) t += red[i];
+  __syncthreads();
+  return t;
+}
+
+// Parallel cyclic Jacobi (round-robin pairing): A <- diag, V <- eigenvectors
+// (columns).  A is symmetric s x s; V must hold the identity on entry.
+__device__ void cta_jacobi(double* A, double* V, int s, int ld, double* red, double* rc, double* rs, int* ra,
+                           int* rb) {
+  const int s2 = s + (s & 1);
+  const int np = s2 / 2;
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
+      const int i = t / s, j = t % s;
+      const double a = A[i * ld + j];
+      if (i == j) dia += a * a; else off += a * a;
+    }
+    off = cta_sum(off, red);
+    dia = cta_sum(dia, red);
+    if (!(off > 1e-32 * (dia + off))) break;
+    for (int r = 0; r < s2 - 1; ++r) {
+      for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        int a, b;
+        if (p == 0) {
+          a = r;
+          b = s2 - 1;
+        } else {
+          a = (r + p) % (s2 - 1);
+          b = (r - p + s2 - 1) % (s2 - 1);
+        }
+        if (a > b) {
+          const int t = a;
+          a = b;
+          b = t;
+        }
+        double c = 1.0, sn = 0.0;
+        if (b < s) {
+          const double apq = A[a * ld + b];
+          const double app = A[a * ld + a], aqq = A[b * ld + b];
+          if (fabs(apq) > 1e-300 && fabs(apq) > DBL_EPSILON * 1e-3 * sqrt(fabs(app * aqq))) {
+            const double theta = (aqq - app) / (2.0 * apq);
+            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            c = 1.0 / sqrt(t * t + 1.0);
+            sn = t * c;
+          }
+        }
+        rc[p] = c;
+        rs[p] = sn;
+        ra[p] = a;
+        rb[p] = b < s ? b : -1;
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < np * s; t += blockDim.x) {
+        const int p = t / s, k = t % s;
+        const int a = ra[p], b = rb[p];
+        if (b < 0 || rs[p] == 0.0) continue;
+        const double x = A[a * ld + k], y = A[b * ld + k];
+        A[a * ld + k] = rc[p] * x - rs[p] * y;
+        A[b * ld + k] = rs[p] * x + rc[p] * y;
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < np * s; t += blockDim.x) {
+        const int p = t / s, k = t % s;
+        const int a = ra[p], b = rb[p];
+        if (b < 0 || rs[p] == 0.0) continue;
+        const double x = A[k * ld + a], y = A[k * ld + b];
+        A[k * ld + a] = rc[p] * x - rs[p] * y;
+        A[k * ld + b] = rs[p] * x + rc[p] * y;
+        const double vx = V[k * ld + a], vy = V[k * ld + b];
+        V[k * ld + a] = rc[p] * vx - rs[p] * vy;
+        V[k * ld + b] = rs[p] * vx + rc[p] * vy;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// order[0..s) = indices of diag(A) ascending (stable); thread 0 only.
+__device__ void sort_eigs(const double* A, int s, int ld, int* order) {
+  for (int i = 0; i < s; ++i) order[i] = i;
+  for (int i = 1; i < s; ++i) {
+    const int v = order[i];
+    const double key = A[v * ld + v];
+    int j = i - 1;
+    while (j >= 0 && A[order[j] * ld + order[j]] > key) {
+      order[j + 1] = order[j];
+      --j;
+    }
+    order[j + 1] = v;
+  }
+}
+
+// Generalised Rayleigh-Ritz on the Gram sub-matrices selected by idx[0..s):
+// (D GA D) y = theta (D GB D) y.  On success Z[0..s) x [0..nsel) holds
+// D L^-T V_sel and theta_out the selected Ritz values.
+__device__ bool cta_rr_general(const double* gb, const double* ga, int P, const int* idx, int s, int nsel,
+                               int largest, double chol_tol, SmallSmem sm, double* dsc, double* theta_out,
+                               double* red, double* rc, double* rs, int* ra, int* rb, int* order, int* sflag) {
+  const int ld = sm.ld;
+  for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
+    const int i = t / s, j = t % s;
+    sm.B[i * ld + j] = gb[idx[i] * P + idx[j]];
+    sm.A[i * ld + j] = ga[idx[i] * P + idx[j]];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int bad = 0;
+    for (int i = 0; i < s; ++i) {
+      const double d = sm.B[i * ld + i];
+      if (!(d > 0.0) || !isfinite(d)) bad = 1;
+      dsc[i] = (d > 0.0) ? 1.0 / sqrt(d) : 0.0;
+    }
+    *sflag = bad;
+  }
+  __syncthreads();
+  if (*sflag) return false;
+  for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
+    const int i = t / s, j = t % s;
+    const double f = dsc[i] * dsc[j];
+    sm.B[i * ld + j] *= f;
+    sm.A[i * ld + j] *= f;
+  }
+  __syncthreads();
+  if (!cta_cholesky(sm.B, s, ld, chol_tol, sflag)) return false;
+  // A <- L^-1 A L^-T
+  cta_trsm_left_lower(sm.B, sm.A, s, s, ld);
+  cta_trsm_right_lowerT(sm.B, sm.A, s, s, ld);
+  // symmetrise
+  for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
+    const int i = t / s, j = t % s;
+    if (i < j) {
+      const double v = 0.5 * (sm.A[i * ld + j] + sm.A[j * ld + i]);
+      sm.A[i * ld + j] = v;
+      sm.A[j * ld + i] = v;
+    }
+  }
+  __syncthreads();
+  cta_identity(sm.V, s, ld);
+  __syncthreads();
+  cta_jacobi(sm.A, sm.V, s, ld, red, rc, rs, ra, rb);
+  if (threadIdx.x == 0) {
+    sort_eigs(sm.A, s, ld, order);
+    if (largest) {
+      for (int i = 0; i < s / 2; ++i) {
+        const int t = order[i];
+        order[i] = order[s - 1 - i];
+        order[s - 1 - i] = t;
+      }
+    }
+    for (int q = 0; q < nsel; ++q) theta_out[q] = sm.A[order[q] * ld + order[q]];
+  }
+  __syncthreads();
+  // Z = V[:, order[0..nsel)]
+  for (int t = threadIdx.x; t < s * nsel; t += blockDim.x) {
+    const int i = t / nsel, q = t % nsel;
+    sm.Z[i * ld + q] = sm.V[i * ld + order[q]];
+  }
+  __syncthreads();
+  cta_trsm_left_lowerT(sm.B, sm.Z, s, nsel, ld);
+  for (int t = threadIdx.x; t < s * nsel; t += blockDim.x) {
+    const int i = t / nsel, q = t % nsel;
+    sm.Z[i * ld + q] *= dsc[i];
+  }
+  __syncthreads();
+  return true;
+}
+
+__global__ void __launch_bounds__(ST) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
+                                                   int mode) {
+  extern __shared__ double smem[];
+  __shared__ double red[ST / 32];
+  __shared__ double rc[SMAX / 2 + 1], rs[SMAX / 2 + 1], dsc[3 * MAXM], theta[MAXM], rn[MAXM];
+  __shared__ int ra[SMAX / 2 + 1], rb[SMAX / 2 + 1], order[3 * MAXM], idx[3 * MAXM];
+  __shared__ int sflag, sdone, s_na, s_withp;
+  const int LDS = 3 * MAXM;
+  SmallSmem sm{smem, smem + LDS * LDS, smem + 2 * LDS * LDS, smem + 3 * LDS * LDS, LDS};
+  const int m = ctrl->m;
+  const int P = ns * m;
+  const double* gb = gram;
+  const double* ga = gram + P * P;
+  if (threadIdx.x == 0) {
+    sdone = ctrl->done;
+    // iterations queued after convergence: the final best copy already happened
+    if (sdone && mode == SM_ITER) ctrl->copy_best = 0;
+  }
+  __syncthreads();
+  if (sdone) return;
+
+  if (mode == SM_INIT) {
+    for (int i = threadIdx.x; i < m; i += blockDim.x) idx[i] = i;
+    __syncthreads();
+    const bool ok = cta_rr_general(gb, ga, P, idx, m, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc,
+                                   rs, ra, rb, order, &sflag);
+    if (threadIdx.x == 0) {
+      ctrl->iter = 0;
+      ctrl->copy_best = 0;
+      ctrl->has_p = 0;
+      ctrl->p_valid = 0;
+      ctrl->best_sum = DBL_MAX;
+      ctrl->best_iter = -1;
+      ctrl->n_active = m;
+      for (int c = 0; c < MAXM; ++c) ctrl->active[c] = c < m ? 1 : 0;
+      if (!ok) {
+        ctrl->done = 1;
+        ctrl->status = ST_BREAKDOWN;
+      } else {
+        for (int q = 0; q < m; ++q) ctrl->lam[q] = theta[q];
+      }
+    }
+    __syncthreads();
+    if (ok) {
+      for (int t = threadIdx.x; t < MAXM * MAXM; t += blockDim.x) {
+        const int i = t / MAXM, q = t % MAXM;
+        ctrl->Cx[t] = (i < m && q < m) ? sm.Z[i * LDS + q] : 0.0;
+        ctrl->Cr[t] = 0.0;
+        ctrl->Cp[t] = 0.0;
+      }
+    }
+    return;
+  }
+
+  if (mode == SM_RR_PLAIN) {
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) sm.A[(t / m) * LDS + t % m] = ga[t];
+    __syncthreads();
+    cta_identity(sm.V, m, LDS);
+    __syncthreads();
+    cta_jacobi(sm.A, sm.V, m, LDS, red, rc, rs, ra, rb);
+    if (threadIdx.x == 0) {
+      sort_eigs(sm.A, m, LDS, order);
+      for (int q = 0; q < m; ++q) ctrl->lam[q] = sm.A[order[q] * LDS + order[q]];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < MAXM * MAXM; t += blockDim.x) {
+      const int i = t / MAXM, q = t % MAXM;
+      ctrl->Cx[t] = (i < m && q < m) ? sm.V[i * LDS + order[q]] : 0.0;
+    }
+    return;
+  }
+
+  if (mode == SM_CHOLQR) {
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) sm.B[(t / m) * LDS + t % m] = gb[t];
+    __syncthreads();
+    const bool ok = cta_cholesky(sm.B, m, LDS, 0.0, &sflag);
+    if (ok) {
+      cta_identity(sm.Z, m, LDS);
+      __syncthreads();
+      cta_trsm_left_lowerT(sm.B, sm.Z, m, m, LDS);
+    }
+    for (int t = threadIdx.x; t < MAXM * MAXM; t += blockDim.x) {
+      const int i = t / MAXM, q = t % MAXM;
+      ctrl->Cx[t] = (ok && i < m && q < m) ? sm.Z[i * LDS + q] : 0.0;
+    }
+    if (threadIdx.x == 0) ctrl->status = ok ? ST_CONVERGED : ST_BREAKDOWN;
+    return;
+  }
+
+  // ---- SM_ITER --------------------------------------------------------------
+  if (threadIdx.x == 0) {
+    const int k = ctrl->k_wanted;
+    double sum = 0.0;
+    for (int c = 0; c < m; ++c) {
+      const double g = gb[(m + c) * P + (m + c)];
+      rn[c] = sqrt(g > 0.0 ? g : 0.0);
+      ctrl->rnorm[c] = rn[c];
+      if (c < k) sum += rn[c];
+    }
+    int copy = 0;
+    if (ctrl->best_sum > sum) {
+      ctrl->best_sum = sum;
+      ctrl->best_iter = ctrl->iter;
+      for (int c = 0; c < m; ++c) {
+        ctrl->best_lam[c] = ctrl->lam[c];
+        ctrl->best_rnorm[c] = rn[c];
+      }
+      copy = 1;
+    }
+    ctrl->copy_best = copy;
+    int na_wanted = 0;
+    for (int c = 0; c < m; ++c) {
+      if (c < k) {
+        ctrl->active[c] = (ctrl->active[c] && rn[c] > ctrl->tol) ? 1 : 0;
+        na_wanted += ctrl->active[c];
+      } else {
+        ctrl->active[c] = 1;
+      }
+    }
+    int done = 0;
+    if (na_wanted == 0) {
+      done = 1;
+      ctrl->status = ST_CONVERGED;
+    } else if (ctrl->iter >= ctrl->maxiter) {
+      done = 1;
+      ctrl->status = ST_MAXITER;
+    }
+    ctrl->done = done;
+    sdone = done;
+    if (!done) ctrl->iter += 1;
+    int na = 0;
+    for (int c = 0; c < m; ++c)
+      if (ctrl->active[c]) idx[m + na++] = m + c;
+    for (int c = 0; c < m; ++c) idx[c] = c;
+    s_na = na;
+    s_withp = ctrl->p_valid;
+  }
+  __syncthreads();
+  if (sdone) return;
+  const int na = s_na;
+  bool ok = false;
+  int withp = s_withp;
+  if (withp) {
+    if (threadIdx.x == 0) {
+      int q = 0;
+      for (int c = 0; c < m; ++c)
+        if (ctrl->active[c]) idx[m + na + q++] = 2 * m + c;
+    }
+    __syncthreads();
+    ok = cta_rr_general(gb, ga, P, idx, m + 2 * na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs,
+                        ra, rb, order, &sflag);
+    if (!ok) withp = 0;
+  }
+  if (!ok) {
+    ok = cta_rr_general(gb, ga, P, idx, m + na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs, ra,
+                        rb, order, &sflag);
+  }
+  if (!ok) {
+    if (threadIdx.x == 0) {
+      ctrl->done = 1;
+      ctrl->status = ST_BREAKDOWN;
+    }
+    return;
+  }
+  // scatter the coefficients
+  for (int t = threadIdx.x; t < MAXM * MAXM; t += blockDim.x) {
+    ctrl->Cx[t] = 0.0;
+    ctrl->Cr[t] = 0.0;
+    ctrl->Cp[t] = 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < (m + na * (withp ? 2 : 1)) * m; t += blockDim.x) {
+    const int row = t / m, q = t % m;
+    const double v = sm.Z[row * LDS + q];
+    const int col = idx[row];
+    if (col < m)
+      ctrl->Cx[col * MAXM + q] = v;
+    else if (col < 2 * m)
+      ctrl->Cr[(col - m) * MAXM + q] = v;
+    else
+      ctrl->Cp[(col - 2 * m) * MAXM + q] = v;
+  }
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < m; ++q) ctrl->lam[q] = theta[q];
+    ctrl->has_p = withp;
+    ctrl->p_valid = 1;
+  }
+}
+
+__global__ void __launch_bounds__(ST) k_small_dense(const double* __restrict__ a, int s, int mode, double* evals,
+                                                    double* evecs) {
+  extern __shared__ double smem[];
+  __shared__ double red[ST / 32];
+  __shared__ double rc[SMAX / 2 + 1], rs[SMAX / 2 + 1];
+  __shared__ int ra[SMAX / 2 + 1], rb[SMAX / 2 + 1], order[SMAX];
+  __shared__ int sflag;
+  const int ld = SMAX;
+  double* A = smem;
+  double* V = smem + SMAX * SMAX;
+  for (int t = threadIdx.x; t < s * s; t += blockDim.x) A[(t / s) * ld + t % s] = a[t];
+  __syncthreads();
+  if (mode == SM_RR_PLAIN) {
+    cta_identity(V, s, ld);
+    __syncthreads();
+    cta_jacobi(A, V, s, ld, red, rc, rs, ra, rb);
+    if (threadIdx.x == 0) {
+      sort_eigs(A, s, ld, order);
+      for (int q = 0; q < s; ++q) evals[q] = A[order[q] * ld + order[q]];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
+      const int i = t / s, q = t % s;
+      evecs[t] = V[i * ld + order[q]];
+    }
+  } else {
+    const bool ok = cta_cholesky(A, s, ld, 0.0, &sflag);
+    if (ok) {
+      cta_identity(V, s, ld);
+      __syncthreads();
+      cta_trsm_left_lowerT(A, V, s, s, ld);
+      for (int t = threadIdx.x; t < s * s; t += blockDim.x) evecs[t] = V[(t / s) * ld + t % s];
+    }
+    if (threadIdx.x == 0) evals[0] = ok ? 1.0 : 0.0;
+  }
+}
+
+}  // namespace
+
+void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode) {
+  const int LDS = 3 * MAXM;
+  const size_t smem = sizeof(double) * 4 * LDS * LDS;
+  static bool attr_set[128] = {};
+  if (ex.device >= 0 && ex.device < 128 && !attr_set[ex.device]) {
+    SI_CUDA(cudaFuncSetAttribute(k_small_step, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    attr_set[ex.device] = true;
+  }
+  k_small_step<<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  SI_LAUNCH_CHECK();
+}
+
+void small_dense_dev(const Exec& ex, const double* a, int s, int mode, double* evals, double* evecs) {
+  SI_REQUIRE(s >= 1 && s <= SMAX, SI_INVALID_ARGUMENT, "small_dense: size out of range");
+  const size_t smem = sizeof(double) * 2 * SMAX * SMAX;
+  static bool attr_set[128] = {};
+  if (ex.device >= 0 && ex.device < 128 && !attr_set[ex.device]) {
+    SI_CUDA(cudaFuncSetAttribute(k_small_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    attr_set[ex.device] = true;
+  }
+  k_small_dense<<<1, ST, smem, ex.stream>>>(a, s, mode, evals, evecs);
+  SI_LAUNCH_CHECK();
+}
+
+}  // namespace si

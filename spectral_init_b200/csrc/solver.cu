@@ -1,0 +1,543 @@
+// Eigensolver drivers: block LOBPCG with the crate's warm-restart wrapper
+// (src/solvers/lobpcg.rs:227-465), the Chebyshev-filtered start (:113-150,
+// :270-291), Rayleigh-Ritz refinement (:158-187), residual gates
+// (src/metrics.rs:57-92), randomized SVD on 2I - L (src/solvers/rsvd.rs:135-213)
+// and the escalation chain (src/solvers/mod.rs:70-224).
+//
+// The LOBPCG iteration runs entirely on the device: per iteration one SpMM
+// (A R), one fused Gram pass over [X R P AX AR AP], one single-CTA small step
+// (locking, convergence, Rayleigh-Ritz) and one fused block update.  Control
+// state (iteration count, active mask, best iterate, done flag) lives in
+// device memory; the host only enqueues batches of iterations and reads the
+// done flag between batches.  Kernels enqueued after convergence exit at
+// their first instruction.
+#include <cfloat>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <numeric>
+#include <type_traits>
+#include <vector>
+
+#include "solver.h"
+
+namespace si {
+
+constexpr double REGULARIZATION_EPS = 1e-5;
+constexpr double CHEB_LOWER_BOUND = 0.1;
+constexpr double CHEB_UPPER_BOUND = 2.0;
+constexpr int CHEB_DEGREE = 8;
+constexpr int64_t CHEB_MIN_N = 1000;
+constexpr int MAX_WARM_RESTARTS = 3;
+constexpr int LOBPCG_INITIAL_MAXITER_CAP = 300;
+constexpr int LOBPCG_RESTART_MAXITER_CAP = 1000;
+constexpr double LOBPCG_ACCEPT_TOL = 1e-5;
+constexpr double DENSE_EVD_QUALITY_THRESHOLD = 1e-6;
+constexpr double LOBPCG_QUALITY_THRESHOLD = 1e-5;
+constexpr double RSVD_QUALITY_THRESHOLD = 1e-2;
+constexpr int64_t DENSE_MAX_N = 8192;  // largest n the device dense EVD accepts
+
+namespace {
+
+int pick_ld(int m) { return m <= 4 ? 4 : (m <= 8 ? 8 : 16); }
+
+// Block width: the wanted k vectors plus guard vectors up to the padded row
+// width when the problem is large enough (guards raise the convergence rate
+// of the wanted pairs at no extra memory traffic: rows are padded anyway).
+int choose_block(int64_t n, int k, int requested) {
+  if (requested > 0) return std::min(std::max(requested, k), MAXM);
+  const int ld = pick_ld(k);
+  if (n >= 64LL * ld) return ld;
+  return k;
+}
+
+template <class XT>
+struct LobpcgState {
+  int64_t n = 0;
+  int ld = 0, m = 0;
+  DevBuf<XT> X, AX, R, AR, P, AP, Xbest;
+  DevBuf<double> gram;
+  DevBuf<LobpcgCtrl> ctrl, aux;
+  GramWork gw;
+  void alloc(const Exec& ex, int64_t n_, int m_, int ld_) {
+    n = n_;
+    m = m_;
+    ld = ld_;
+    const size_t sz = static_cast<size_t>(n) * ld;
+    X.alloc(sz, ex.stream);
+    AX.alloc(sz, ex.stream);
+    R.alloc(sz, ex.stream);
+    AR.alloc(sz, ex.stream);
+    P.alloc(sz, ex.stream);
+    AP.alloc(sz, ex.stream);
+    Xbest.alloc(sz, ex.stream);
+    gram.alloc(2 * (3 * MAXM) * (3 * MAXM), ex.stream);
+    ctrl.alloc(1, ex.stream);
+    aux.alloc(1, ex.stream);
+  }
+  const int* stop() const { return &ctrl.get()->done; }
+  LobpcgBlocks<XT> blocks() {
+    return LobpcgBlocks<XT>{X.get(), R.get(), P.get(), AX.get(), AR.get(), AP.get(), Xbest.get()};
+  }
+};
+
+struct CoreOutcome {
+  int status = ST_BREAKDOWN;
+  int iterations = 0;
+  bool best_valid = false;
+  double best_lam[MAXM] = {};
+  double best_rnorm[MAXM] = {};
+};
+
+template <class XT>
+CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int k_wanted, double tol, int maxiter,
+                        bool largest, double chol_tol, bool f32vals, int& spmm_calls) {
+  LobpcgCtrl h;
+  std::memset(&h, 0, sizeof(h));
+  h.m = s.m;
+  h.k_wanted = k_wanted;
+  h.maxiter = maxiter;
+  h.largest = largest ? 1 : 0;
+  h.tol = tol;
+  h.chol_tol = chol_tol;
+  h.best_sum = DBL_MAX;
+  SI_CUDA(cudaMemcpyAsync(s.ctrl.get(), &h, sizeof(h), cudaMemcpyHostToDevice, ex.stream));
+  s.P.zero();
+  s.AP.zero();
+  s.R.zero();
+  s.AR.zero();
+  Epilogue<XT> ep;
+  spmm_dev<XT>(ex, A, s.X.get(), s.AX.get(), s.ld, s.m, ep, nullptr, f32vals);
+  ++spmm_calls;
+  {
+    const XT* blk[2] = {s.X.get(), s.AX.get()};
+    gram_dev<XT>(ex, s.gw, GRAM_SYM2, blk, 1, 2, s.m, s.ld, s.n, s.gram.get());
+  }
+  small_step_dev(ex, s.ctrl.get(), s.gram.get(), 1, SM_INIT);
+  lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 1);
+  const XT* blk6[6] = {s.X.get(), s.R.get(), s.P.get(), s.AX.get(), s.AR.get(), s.AP.get()};
+  int batch = 4;
+  int launched = 0;
+  for (;;) {
+    for (int b = 0; b < batch; ++b) {
+      spmm_dev<XT>(ex, A, s.R.get(), s.AR.get(), s.ld, s.m, ep, s.stop(), f32vals);
+      gram_dev<XT>(ex, s.gw, GRAM_SYM2, blk6, 3, 6, s.m, s.ld, s.n, s.gram.get(), s.stop());
+      small_step_dev(ex, s.ctrl.get(), s.gram.get(), 3, SM_ITER);
+      lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 0);
+    }
+    launched += batch;
+    int done = 0;
+    SI_CUDA(cudaMemcpyAsync(&done, s.stop(), sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
+    if (done) break;
+    SI_REQUIRE(launched <= maxiter + 8, SI_CUDA_ERROR, "lobpcg: device loop did not terminate");
+    batch = std::min(batch * 2, 32);
+  }
+  SI_CUDA(cudaMemcpyAsync(&h, s.ctrl.get(), sizeof(h), cudaMemcpyDeviceToHost, ex.stream));
+  SI_CUDA(cudaStreamSynchronize(ex.stream));
+  CoreOutcome o;
+  o.status = h.status;
+  o.iterations = h.iter;
+  spmm_calls += h.iter;
+  o.best_valid = h.best_iter >= 0 && h.best_sum < DBL_MAX;
+  for (int c = 0; c < s.m; ++c) {
+    o.best_lam[c] = h.best_lam[c];
+    o.best_rnorm[c] = h.best_rnorm[c];
+  }
+  return o;
+}
+
+// (X0 + T_8((L - cI)/e) X0) / 2 with unit columns, in place in s.X.
+template <class XT>
+void chebyshev_start(const Exec& ex, const OpDev& L, LobpcgState<XT>& s, bool f32vals, int& spmm_calls) {
+  const double a = CHEB_LOWER_BOUND, b = CHEB_UPPER_BOUND;
+  const double c = (a + b) / 2.0, e = (b - a) / 2.0;
+  const double scale = 2.0 / e, shift = scale * c;
+  XT* bufs[3] = {s.R.get(), s.AR.get(), s.P.get()};
+  Epilogue<XT> ep1;
+  ep1.alpha = 1.0 / e;
+  ep1.beta = -c / e;
+  ep1.z1 = s.X.get();
+  spmm_dev<XT>(ex, L, s.X.get(), bufs[0], s.ld, s.m, ep1, nullptr, f32vals);
+  ++spmm_calls;
+  const XT* yprev = s.X.get();
+  XT* y = bufs[0];
+  int nxt = 1;
+  for (int d = 2; d <= CHEB_DEGREE; ++d) {
+    XT* out = bufs[nxt];
+    Epilogue<XT> ep;
+    ep.alpha = scale;
+    ep.beta = -shift;
+    ep.z1 = y;
+    ep.gamma = -1.0;
+    ep.z2 = yprev;
+    if (d == CHEB_DEGREE) {
+      ep.alpha *= 0.5;
+      ep.beta *= 0.5;
+      ep.gamma = -0.5;
+      ep.delta = 0.5;
+      ep.z3 = s.X.get();
+    }
+    spmm_dev<XT>(ex, L, y, out, s.ld, s.m, ep, nullptr, f32vals);
+    ++spmm_calls;
+    yprev = y;
+    y = out;
+    nxt = (nxt + 1) % 3;
+  }
+  DevBuf<double> norms(MAXM, ex.stream);
+  column_residual_norms_dev<XT>(ex, s.gw, y, nullptr, nullptr, s.m, s.ld, s.n, norms.get());
+  double hn[MAXM];
+  SI_CUDA(cudaMemcpyAsync(hn, norms.get(), sizeof(double) * s.m, cudaMemcpyDeviceToHost, ex.stream));
+  SI_CUDA(cudaStreamSynchronize(ex.stream));
+  double sc[MAXM];
+  for (int j = 0; j < s.m; ++j) sc[j] = hn[j] > 1e-300 ? 1.0 / hn[j] : 1.0;
+  SI_CUDA(cudaMemcpyAsync(norms.get(), sc, sizeof(double) * s.m, cudaMemcpyHostToDevice, ex.stream));
+  SI_CUDA(cudaMemcpyAsync(s.X.get(), y, sizeof(XT) * s.n * s.ld, cudaMemcpyDeviceToDevice, ex.stream));
+  scale_columns_dev<XT>(ex, s.X.get(), s.n, s.m, s.ld, norms.get());
+  SI_CUDA(cudaStreamSynchronize(ex.stream));
+}
+
+// Rayleigh-Ritz of the operator on span(src): dst = src V, vals = theta.
+void rr_refine(const Exec& ex, const OpDev& L, LobpcgState<double>& s, const double* src, double* dst,
+               std::vector<double>& vals, int& spmm_calls) {
+  Epilogue<double> ep;
+  spmm_dev<double>(ex, L, src, s.AX.get(), s.ld, s.m, ep);
+  ++spmm_calls;
+  const double* blk[2] = {src, s.AX.get()};
+  gram_dev<double>(ex, s.gw, GRAM_SYM2, blk, 1, 2, s.m, s.ld, s.n, s.gram.get());
+  LobpcgCtrl h;
+  std::memset(&h, 0, sizeof(h));
+  h.m = s.m;
+  SI_CUDA(cudaMemcpyAsync(s.aux.get(), &h, sizeof(h), cudaMemcpyHostToDevice, ex.stream));
+  small_step_dev(ex, s.aux.get(), s.gram.get(), 1, SM_RR_PLAIN);
+  const double* in[1] = {src};
+  const double* coef[1] = {s.aux.get()->Cx};
+  combine_dev<double>(ex, in, coef, 1, dst, s.m, s.m, MAXM, s.ld, s.n);
+  SI_CUDA(cudaMemcpyAsync(&h, s.aux.get(), sizeof(h), cudaMemcpyDeviceToHost, ex.stream));
+  SI_CUDA(cudaStreamSynchronize(ex.stream));
+  vals.assign(h.lam, h.lam + s.m);
+}
+
+}  // namespace
+
+std::vector<double> eigenpair_residuals_dev(const Exec& ex, const OpDev& op, const double* vecs, int ld,
+                                            const std::vector<double>& vals, int k, double floor) {
+  SI_REQUIRE(k <= MAXM, SI_INVALID_ARGUMENT, "residuals: too many vectors");
+  const int64_t n = op.n;
+  DevBuf<double> ax(static_cast<size_t>(n) * ld, ex.stream), lam(MAXM, ex.stream), rn(MAXM, ex.stream),
+      xn(MAXM, ex.stream);
+  GramWork gw;
+  Epilogue<double> ep;
+  spmm_dev<double>(ex, op, vecs, ax.get(), ld, k, ep);
+  SI_CUDA(cudaMemcpyAsync(lam.get(), vals.data(), sizeof(double) * k, cudaMemcpyHostToDevice, ex.stream));
+  column_residual_norms_dev<double>(ex, gw, ax.get(), vecs, lam.get(), k, ld, n, rn.get());
+  column_residual_norms_dev<double>(ex, gw, vecs, nullptr, nullptr, k, ld, n, xn.get());
+  double hr[MAXM], hx[MAXM];
+  SI_CUDA(cudaMemcpyAsync(hr, rn.get(), sizeof(double) * k, cudaMemcpyDeviceToHost, ex.stream));
+  SI_CUDA(cudaMemcpyAsync(hx, xn.get(), sizeof(double) * k, cudaMemcpyDeviceToHost, ex.stream));
+  SI_CUDA(cudaStreamSynchronize(ex.stream));
+  std::vector<double> out(k);
+  for (int c = 0; c < k; ++c) out[c] = hr[c] / std::max(hx[c], floor);
+  return out;
+}
+
+double max_eigenpair_residual_dev(const Exec& ex, const OpDev& op, const EigenResult& r) {
+  const std::vector<double> res = eigenpair_residuals_dev(ex, op, r.vecs.get(), r.k, r.vals, r.k, 1e-300);
+  double acc = 0.0;
+  for (double v : res) {
+    if (std::isnan(acc) || std::isnan(v)) acc = NAN;
+    else acc = std::max(acc, v);
+  }
+  return acc;
+}
+
+bool lobpcg_solve_dev(const Exec& ex, const OpDev& op, int n_components, uint64_t seed, bool regularize,
+                      const double* sqrt_deg, const SolverConfig& cfg, EigenResult& out, SolverStats& st) {
+  const int64_t n = op.n;
+  const int k = n_components + 1;
+  if (n_components <= 0 || k >= n) return false;
+  SI_REQUIRE(k <= MAXM, SI_INVALID_ARGUMENT, "lobpcg: n_components + 1 must be <= 16");
+  const int m = choose_block(n, k, cfg.block_size);
+  const int ld = pick_ld(m);
+  const bool mixed = cfg.precision == SI_PRECISION_MIXED && op.v32 != nullptr;
+  OpDev A = op;
+  if (regularize) A.diag += REGULARIZATION_EPS;
+
+  LobpcgState<double> s;
+  s.alloc(ex, n, m, ld);
+  if (cfg.warm_start != nullptr) {
+    SI_CUDA(cudaMemsetAsync(s.X.get(), 0, sizeof(double) * n * ld, ex.stream));
+    std::vector<int> cols(std::min(m, cfg.warm_start_ld));
+    std::iota(cols.begin(), cols.end(), 0);
+    gather_columns_dev<double, double>(ex, cfg.warm_start, cfg.warm_start_ld, s.X.get(), ld, n, cols);
+  } else {
+    fill_normal_dev<double>(ex, s.X.get(), n, m, ld, seed, 1);
+    set_column_normalized_dev<double>(ex, s.gw, s.X.get(), ld, n, sqrt_deg);
+  }
+
+  const double tol32 = static_cast<double>(static_cast<float>(LOBPCG_ACCEPT_TOL));  // linfa takes tol as f32
+  std::vector<int> all_cols(m);
+  std::iota(all_cols.begin(), all_cols.end(), 0);
+
+  if (mixed) {
+    // f32 bulk: Chebyshev filter and LOBPCG on f32 blocks and f32 matrix
+    // values (f64 accumulation, f64 Gram and small steps), then the f64
+    // passes below finish from the f32 iterate.
+    LobpcgState<float> s32;
+    s32.alloc(ex, n, m, ld);
+    gather_columns_dev<double, float>(ex, s.X.get(), ld, s32.X.get(), ld, n, all_cols);
+    if (n >= CHEB_MIN_N) chebyshev_start<float>(ex, A, s32, true, st.spmm_calls);
+    const double switch_tol = cfg.mixed_switch_tol > 0.0 ? cfg.mixed_switch_tol : 1e-4;
+    const int maxiter32 = static_cast<int>(std::min<int64_t>(5 * n, cfg.max_iterations > 0 ? cfg.max_iterations
+                                                                                           : LOBPCG_RESTART_MAXITER_CAP));
+    CoreOutcome o32 = lobpcg_core<float>(ex, A, s32, k, switch_tol, maxiter32, false, 1e-10, true, st.spmm_calls);
+    st.fp32_iterations += o32.iterations;
+    st.iterations += o32.iterations;
+    if (o32.best_valid) {
+      gather_columns_dev<float, double>(ex, s32.Xbest.get(), ld, s.X.get(), ld, n, all_cols);
+    } else {
+      gather_columns_dev<float, double>(ex, s32.X.get(), ld, s.X.get(), ld, n, all_cols);
+    }
+  } else if (n >= CHEB_MIN_N) {
+    chebyshev_start<double>(ex, A, s, false, st.spmm_calls);
+  }
+
+  DevBuf<double> last(static_cast<size_t>(n) * ld, ex.stream);
+  std::vector<double> last_vals;
+  bool have_last = false;
+  int restart_count = 0;
+  for (int restart = 0; restart <= MAX_WARM_RESTARTS; ++restart) {
+    int cap = restart == 0 ? LOBPCG_INITIAL_MAXITER_CAP : LOBPCG_RESTART_MAXITER_CAP;
+    if (cfg.max_iterations > 0) cap = cfg.max_iterations;
+    const int maxiter = static_cast<int>(std::min<int64_t>(5 * n, cap));
+    CoreOutcome o = lobpcg_core<double>(ex, A, s, k, tol32, maxiter, false, 1e-14, false, st.spmm_calls);
+    st.iterations += o.iterations;
+    if (!o.best_valid) break;  // breakdown before any iterate: the crate's Err((_, None))
+    bool accept = o.status == ST_CONVERGED;
+    if (!accept) {
+      accept = true;
+      for (int c = 0; c < k; ++c) accept = accept && (o.best_rnorm[c] < LOBPCG_ACCEPT_TOL);
+    }
+    if (!accept) {
+      if (restart < MAX_WARM_RESTARTS) {
+        SI_CUDA(cudaMemcpyAsync(s.X.get(), s.Xbest.get(), sizeof(double) * n * ld, cudaMemcpyDeviceToDevice,
+                                ex.stream));
+        continue;
+      }
+      break;
+    }
+    std::vector<double> vals;
+    rr_refine(ex, op, s, s.Xbest.get(), s.X.get(), vals, st.spmm_calls);
+    const std::vector<double> res = eigenpair_residuals_dev(ex, op, s.X.get(), ld, vals, k, DBL_EPSILON);
+    ++st.spmm_calls;
+    bool ok = true;
+    for (int c = 0; c < k; ++c) ok = ok && (res[c] < LOBPCG_ACCEPT_TOL);
+    if (ok) {
+      out.k = k;
+      out.vals.assign(vals.begin(), vals.begin() + k);
+      out.vecs.alloc(static_cast<size_t>(n) * k, ex.stream);
+      gather_columns_dev<double, double>(ex, s.X.get(), ld, out.vecs.get(), k, n,
+                                         std::vector<int>(all_cols.begin(), all_cols.begin() + k));
+      st.restarts = restart_count;
+      return true;
+    }
+    ++restart_count;
+    SI_CUDA(cudaMemcpyAsync(last.get(), s.X.get(), sizeof(double) * n * ld, cudaMemcpyDeviceToDevice, ex.stream));
+    last_vals = vals;
+    have_last = true;
+  }
+  st.restarts = restart_count;
+  if (!have_last) return false;
+  out.k = k;
+  out.vals.assign(last_vals.begin(), last_vals.begin() + k);
+  out.vecs.alloc(static_cast<size_t>(n) * k, ex.stream);
+  gather_columns_dev<double, double>(ex, last.get(), ld, out.vecs.get(), k, n,
+                                     std::vector<int>(all_cols.begin(), all_cols.begin() + k));
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Randomized SVD on M = 2I - L.
+namespace {
+
+// Orthonormalise the columns of Y [n x K] in place (CholQR2, shifted CholQR
+// when the Gram matrix is numerically singular).
+void cholqr_dev(const Exec& ex, GramWork& gw, double* y, double* tmp, int K, int ld, int64_t n) {
+  DevBuf<double> g(static_cast<size_t>(K) * K, ex.stream), rinv(static_cast<size_t>(K) * K, ex.stream),
+      flag(SMAX, ex.stream);
+  int plain_passes = 0, shifted_passes = 0;
+  while (plain_passes < 2) {
+    const double* blk[2] = {y, y};
+    gram_dev<double>(ex, gw, GRAM_FULL, blk, 1, 2, K, ld, n, g.get());
+    small_dense_dev(ex, g.get(), K, SM_CHOLQR, flag.get(), rinv.get());
+    double ok = 0.0;
+    SI_CUDA(cudaMemcpyAsync(&ok, flag.get(), sizeof(double), cudaMemcpyDeviceToHost, ex.stream));
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
+    if (ok != 0.0) {
+      ++plain_passes;
+    } else {
+      // shifted CholeskyQR (Fukaya, Kannan, Nakatsukasa, Zhang, Yamamoto 2020): factor G + s I
+      SI_REQUIRE(shifted_passes < 3, SI_CONVERGENCE_FAILURE, "rsvd: orthonormalisation failed");
+      ++shifted_passes;
+      std::vector<double> hg(static_cast<size_t>(K) * K);
+      SI_CUDA(cudaMemcpyAsync(hg.data(), g.get(), sizeof(double) * K * K, cudaMemcpyDeviceToHost, ex.stream));
+      SI_CUDA(cudaStreamSynchronize(ex.stream));
+      double tr = 0.0;
+      for (int i = 0; i < K; ++i) tr += std::fabs(hg[static_cast<size_t>(i) * K + i]);
+      const double shift = 11.0 * (static_cast<double>(n) * K + K * (K + 1.0)) * DBL_EPSILON * std::max(tr, 1e-300);
+      for (int i = 0; i < K; ++i) hg[static_cast<size_t>(i) * K + i] += shift;
+      SI_CUDA(cudaMemcpyAsync(g.get(), hg.data(), sizeof(double) * K * K, cudaMemcpyHostToDevice, ex.stream));
+      small_dense_dev(ex, g.get(), K, SM_CHOLQR, flag.get(), rinv.get());
+      SI_CUDA(cudaMemcpyAsync(&ok, flag.get(), sizeof(double), cudaMemcpyDeviceToHost, ex.stream));
+      SI_CUDA(cudaStreamSynchronize(ex.stream));
+      SI_REQUIRE(ok != 0.0, SI_CONVERGENCE_FAILURE, "rsvd: orthonormalisation failed");
+      plain_passes = 0;
+    }
+    const double* in[1] = {y};
+    const double* coef[1] = {rinv.get()};
+    combine_dev<double>(ex, in, coef, 1, tmp, K, K, K, ld, n);
+    SI_CUDA(cudaMemcpyAsync(y, tmp, sizeof(double) * n * ld, cudaMemcpyDeviceToDevice, ex.stream));
+  }
+}
+
+int rsvd_k_sub(int64_t n, int rank) {
+  const int64_t over = std::min<int64_t>(std::max<int64_t>(n / 10, std::max(rank, 5)), std::max<int64_t>(n - rank, 0));
+  return static_cast<int>(std::min<int64_t>(rank + over, n));
+}
+
+}  // namespace
+
+void rsvd_solve_dev(const Exec& ex, const OpDev& op, int n_components, uint64_t seed, int oversampling, int nbiter,
+                    EigenResult& out, SolverStats& st) {
+  const int64_t n = op.n;
+  SI_REQUIRE(n_components > 0 && n_components < n, SI_INVALID_ARGUMENT, "rsvd: need 0 < n_components < n");
+  const int rank = n_components + 1;
+  SI_REQUIRE(rank <= MAXM, SI_INVALID_ARGUMENT, "rsvd: n_components + 1 must be <= 16");
+  int K = oversampling < 0 ? rsvd_k_sub(n, rank) : static_cast<int>(std::min<int64_t>(rank + oversampling, n));
+  K = std::min(K, SMAX);  // device subspace cap
+  if (nbiter <= 0) nbiter = 2;
+  const int ld = K <= 4 ? 4 : (K <= 8 ? 8 : (K <= 16 ? 16 : K));
+  GramWork gw;
+  DevBuf<double> om(static_cast<size_t>(n) * ld, ex.stream), y(static_cast<size_t>(n) * ld, ex.stream),
+      tmp(static_cast<size_t>(n) * ld, ex.stream);
+  fill_normal_dev<double>(ex, om.get(), n, K, ld, seed, 2);
+  Epilogue<double> mep;  // M x = 2 x - A x
+  mep.alpha = -1.0;
+  mep.beta = 2.0;
+  auto apply_m = [&](const double* x, double* yy) {
+    mep.z1 = x;
+    spmm_dev<double>(ex, op, x, yy, ld, K, mep);
+    ++st.spmm_calls;
+  };
+  for (int it = 0; it < nbiter; ++it) {
+    apply_m(om.get(), y.get());
+    cholqr_dev(ex, gw, y.get(), tmp.get(), K, ld, n);
+    apply_m(y.get(), om.get());
+    cholqr_dev(ex, gw, om.get(), tmp.get(), K, ld, n);
+  }
+  apply_m(om.get(), y.get());
+  cholqr_dev(ex, gw, y.get(), tmp.get(), K, ld, n);  // y = Q
+  apply_m(y.get(), om.get());                        // om = M Q
+  DevBuf<double> b(static_cast<size_t>(K) * K, ex.stream), ev(SMAX, ex.stream), ub(static_cast<size_t>(K) * K, ex.stream);
+  const double* blk[2] = {y.get(), om.get()};
+  gram_dev<double>(ex, gw, GRAM_FULL, blk, 1, 2, K, ld, n, b.get());
+  small_dense_dev(ex, b.get(), K, SM_RR_PLAIN, ev.get(), ub.get());
+  const double* in[1] = {y.get()};
+  const double* coef[1] = {ub.get()};
+  combine_dev<double>(ex, in, coef, 1, tmp.get(), K, K, K, ld, n);  // V = Q U_B
+  std::vector<double> mev(K);
+  SI_CUDA(cudaMemcpyAsync(mev.data(), ev.get(), sizeof(double) * K, cudaMemcpyDeviceToHost, ex.stream));
+  SI_CUDA(cudaStreamSynchronize(ex.stream));
+  std::vector<int> cols;
+  std::vector<double> vals;
+  cols.push_back(K - 1);
+  vals.push_back(2.0 - mev[K - 1]);
+  for (int i = 0; i < n_components; ++i) {
+    const int idx = std::max(K - 2 - i, 0);
+    cols.push_back(idx);
+    vals.push_back(2.0 - mev[idx]);
+  }
+  out.k = rank;
+  out.vals = vals;
+  out.vecs.alloc(static_cast<size_t>(n) * rank, ex.stream);
+  gather_columns_dev<double, double>(ex, tmp.get(), ld, out.vecs.get(), rank, n, cols);
+}
+
+// ---------------------------------------------------------------------------
+void dense_evd_result(const Exec& ex, const OpDev& op, int k, EigenResult& out) {
+  SI_REQUIRE(k <= op.n, SI_TOO_FEW_NODES, "dense_evd: k > n");
+  SI_REQUIRE(op.n <= DENSE_MAX_N, SI_CONVERGENCE_FAILURE, "dense_evd: n exceeds the device dense limit");
+  out.k = k;
+  out.vals.assign(k, 0.0);
+  out.vecs.alloc(static_cast<size_t>(op.n) * k, ex.stream);
+  dense_evd_dev(ex, op, k, out.vals.data(), out.vecs.get(), k);
+}
+
+void solve_eigenproblem_dev(const Exec& ex, const OpDev& op, int n_components, uint64_t seed, const double* sqrt_deg,
+                            const SolverConfig& cfg, EigenResult& out, SolverStats& st) {
+  const int64_t n = op.n;
+  const int k = n_components + 1;
+  const int fl = cfg.force_level;
+  auto want = [&](int level) { return fl < 0 || fl == level; };
+  if (want(0) && (n < cfg.dense_threshold || fl == 0) && n <= DENSE_MAX_N) {
+    EigenResult r;
+    dense_evd_result(ex, op, k, r);
+    const double q = max_eigenpair_residual_dev(ex, op, r);
+    if (q < DENSE_EVD_QUALITY_THRESHOLD || fl == 0) {
+      st.level = 0;
+      st.max_residual = q;
+      out = std::move(r);
+      return;
+    }
+  }
+  if (want(1)) {
+    EigenResult r;
+    if (lobpcg_solve_dev(ex, op, n_components, seed, false, sqrt_deg, cfg, r, st)) {
+      const double q = max_eigenpair_residual_dev(ex, op, r);
+      if (q < LOBPCG_QUALITY_THRESHOLD || fl == 1) {
+        st.level = 1;
+        st.max_residual = q;
+        out = std::move(r);
+        return;
+      }
+    }
+  }
+  // Level 2 (shift-invert LOBPCG with a sparse Cholesky factor) has no device
+  // implementation; the chain continues with Level 3.
+  if (want(3)) {
+    EigenResult r;
+    if (lobpcg_solve_dev(ex, op, n_components, seed, true, sqrt_deg, cfg, r, st)) {
+      const double q = max_eigenpair_residual_dev(ex, op, r);
+      if (q < LOBPCG_QUALITY_THRESHOLD || fl == 3) {
+        st.level = 3;
+        st.max_residual = q;
+        out = std::move(r);
+        return;
+      }
+    }
+  }
+  if (want(4)) {
+    EigenResult r;
+    rsvd_solve_dev(ex, op, n_components, seed, cfg.rsvd_oversampling, cfg.rsvd_nbiter, r, st);
+    const double q = max_eigenpair_residual_dev(ex, op, r);
+    if (q < RSVD_QUALITY_THRESHOLD || fl == 4) {
+      st.level = 4;
+      st.max_residual = q;
+      out = std::move(r);
+      return;
+    }
+  }
+  if (want(5)) {
+    SI_REQUIRE(n <= DENSE_MAX_N, SI_CONVERGENCE_FAILURE,
+               "eigensolver failed to converge after full escalation chain (graph too large for the dense fallback)");
+    EigenResult r;
+    dense_evd_result(ex, op, k, r);
+    st.level = 5;
+    st.max_residual = max_eigenpair_residual_dev(ex, op, r);
+    out = std::move(r);
+    return;
+  }
+  throw Error(SI_CONVERGENCE_FAILURE, "eigensolver failed to converge at the requested level");
+}
+
+}  // namespace si

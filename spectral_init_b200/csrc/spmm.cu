@@ -1,0 +1,304 @@
+// CSR SpMM over row-major blocks of vectors: the LinearOperator::apply of the
+// crate (src/operator.rs:176-223) re-designed for sm_100a.
+//
+// Layout: the operator is CSR (u64 indptr, u32 indices, f64 or f32 values)
+// with an optional implicit diagonal coefficient; x and y are row-major
+// [n x ld] blocks, ld in {4, 8, 16} for the vectorised kernels.
+//
+// Mapping: G lanes (4..32, chosen from the mean row length) own one row.
+// Each lane walks the row's entries with stride G, so the index/value
+// streams are read coalesced and with the evict-first L2 policy (they are
+// touched once per SpMM), while the gathered x rows are 32-byte (f64, ld=4)
+// or 16/32-byte (f32) vector loads that stay cached.  The per-lane partial
+// sums are combined by a transposing butterfly: at every step a lane keeps
+// half of its columns and trades the other half, so ld columns cost ld
+// shuffles instead of ld*log2(G), and each lane ends owning distinct output
+// columns that it finishes with the fused epilogue
+//   y = alpha * (diag * x_i + sum_j v_ij x_j) + beta z1 + gamma z2 + delta z3.
+// Accumulation is always f64 (also for f32 data).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "si_internal.h"
+
+namespace si {
+namespace {
+
+template <class T>
+__device__ __forceinline__ T ld_stream(const T* p) {
+  return __ldcs(p);
+}
+
+// Vector gather of one x row of LD elements into f64 registers.
+template <class XT, int LD>
+struct RowLoad;
+
+template <int LD>
+struct RowLoad<double, LD> {
+  __device__ __forceinline__ static void run(const double* p, double (&v)[LD]) {
+#pragma unroll
+    for (int q = 0; q < LD / 4; ++q) {
+      double a, b, c, d;
+      asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+                   : "=d"(a), "=d"(b), "=d"(c), "=d"(d)
+                   : "l"(p + 4 * q));
+      v[4 * q + 0] = a;
+      v[4 * q + 1] = b;
+      v[4 * q + 2] = c;
+      v[4 * q + 3] = d;
+    }
+  }
+};
+
+template <>
+struct RowLoad<float, 4> {
+  __device__ __forceinline__ static void run(const float* p, double (&v)[4]) {
+    float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  }
+};
+
+template <int LD>
+struct RowLoadF32x8 {
+  __device__ __forceinline__ static void run(const float* p, double (&v)[LD]) {
+#pragma unroll
+    for (int q = 0; q < LD / 8; ++q) {
+      float a[8];
+      asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                   : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3]), "=f"(a[4]), "=f"(a[5]), "=f"(a[6]),
+                     "=f"(a[7])
+                   : "l"(p + 8 * q));
+#pragma unroll
+      for (int t = 0; t < 8; ++t) v[8 * q + t] = a[t];
+    }
+  }
+};
+template <>
+struct RowLoad<float, 8> : RowLoadF32x8<8> {};
+template <>
+struct RowLoad<float, 16> : RowLoadF32x8<16> {};
+
+// Transposing butterfly over a group of G lanes.  On return the lane holds
+// W = max(LD/G, 1) column sums starting at the returned base column.
+template <int LD, int G>
+struct GroupReduce {
+  static constexpr int W = (LD >= G) ? LD / G : 1;
+  __device__ __forceinline__ static int run(double (&v)[LD], int sub, unsigned mask) {
+    int base = 0;
+    int width = LD;
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) {
+      if (width > W) {
+        const int h = width / 2;
+        const bool upper = (sub & o) != 0;
+#pragma unroll
+        for (int c = 0; c < LD / 2; ++c) {
+          if (c < h) {
+            const double send = upper ? v[c] : v[c + h];
+            const double keep = upper ? v[c + h] : v[c];
+            v[c] = keep + __shfl_xor_sync(mask, send, o, G);
+          }
+        }
+        if (upper) base += h;
+        width = h;
+      } else {
+#pragma unroll
+        for (int c = 0; c < W; ++c) v[c] += __shfl_xor_sync(mask, v[c], o, G);
+      }
+    }
+    return base;
+  }
+};
+
+template <class VT, class XT, int LD, int G>
+__global__ void __launch_bounds__(256) k_spmm_vec(int64_t n, const uint64_t* __restrict__ indptr,
+                                                  const uint32_t* __restrict__ indices,
+                                                  const VT* __restrict__ vals, double diag,
+                                                  const XT* __restrict__ x, XT* __restrict__ y,
+                                                  Epilogue<XT> ep, const int* __restrict__ stop) {
+  if (stop != nullptr && *stop != 0) return;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane & (G - 1);
+  const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+  const int64_t group = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G;
+  const int64_t ngroups = static_cast<int64_t>(gridDim.x) * blockDim.x / G;
+  constexpr int W = GroupReduce<LD, G>::W;
+  const bool writer = (LD >= G) || ((sub & ((G / (LD < G ? LD : G)) - 1)) == 0);
+
+  for (int64_t row = group; row < n; row += ngroups) {
+    const uint64_t s = indptr[row];
+    const uint64_t e = indptr[row + 1];
+    double acc[LD];
+#pragma unroll
+    for (int c = 0; c < LD; ++c) acc[c] = 0.0;
+    uint64_t k = s + sub;
+    // two entries in flight per lane
+    for (; k + G < e; k += 2 * G) {
+      const uint32_t j0 = ld_stream(indices + k);
+      const uint32_t j1 = ld_stream(indices + k + G);
+      const double v0 = static_cast<double>(ld_stream(vals + k));
+      const double v1 = static_cast<double>(ld_stream(vals + k + G));
+      double x0[LD], x1[LD];
+      RowLoad<XT, LD>::run(x + static_cast<int64_t>(j0) * LD, x0);
+      RowLoad<XT, LD>::run(x + static_cast<int64_t>(j1) * LD, x1);
+#pragma unroll
+      for (int c = 0; c < LD; ++c) acc[c] = fma(v0, x0[c], acc[c]);
+#pragma unroll
+      for (int c = 0; c < LD; ++c) acc[c] = fma(v1, x1[c], acc[c]);
+    }
+    if (k < e) {
+      const uint32_t j0 = ld_stream(indices + k);
+      const double v0 = static_cast<double>(ld_stream(vals + k));
+      double x0[LD];
+      RowLoad<XT, LD>::run(x + static_cast<int64_t>(j0) * LD, x0);
+#pragma unroll
+      for (int c = 0; c < LD; ++c) acc[c] = fma(v0, x0[c], acc[c]);
+    }
+    const int base = GroupReduce<LD, G>::run(acc, sub, mask);
+    if (writer) {
+#pragma unroll
+      for (int c = 0; c < W; ++c) {
+        const int64_t off = row * LD + base + c;
+        double r = fma(diag, static_cast<double>(x[off]), acc[c]);
+        r *= ep.alpha;
+        if (ep.z1) r = fma(ep.beta, static_cast<double>(ep.z1[off]), r);
+        if (ep.z2) r = fma(ep.gamma, static_cast<double>(ep.z2[off]), r);
+        if (ep.z3) r = fma(ep.delta, static_cast<double>(ep.z3[off]), r);
+        y[off] = static_cast<XT>(r);
+      }
+    }
+  }
+}
+
+// Generic kernel: any row stride ld, first k columns, four columns per pass.
+template <class VT, class XT, int G>
+__global__ void __launch_bounds__(256) k_spmm_generic(int64_t n, const uint64_t* __restrict__ indptr,
+                                                      const uint32_t* __restrict__ indices,
+                                                      const VT* __restrict__ vals, double diag,
+                                                      const XT* __restrict__ x, XT* __restrict__ y, int ld,
+                                                      int k, Epilogue<XT> ep, const int* __restrict__ stop) {
+  if (stop != nullptr && *stop != 0) return;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane & (G - 1);
+  const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+  const int64_t group = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G;
+  const int64_t ngroups = static_cast<int64_t>(gridDim.x) * blockDim.x / G;
+  for (int64_t row = group; row < n; row += ngroups) {
+    const uint64_t s = indptr[row];
+    const uint64_t e = indptr[row + 1];
+    for (int c0 = 0; c0 < k; c0 += 4) {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (uint64_t q = s + sub; q < e; q += G) {
+        const int64_t j = ld_stream(indices + q);
+        const double v = static_cast<double>(ld_stream(vals + q));
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (c0 + c < k) acc[c] = fma(v, static_cast<double>(__ldg(x + j * ld + c0 + c)), acc[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int o = G / 2; o >= 1; o >>= 1) acc[c] += __shfl_xor_sync(mask, acc[c], o, G);
+      if (sub < 4 && c0 + sub < k) {
+        double a = acc[0];
+#pragma unroll
+        for (int c = 1; c < 4; ++c)
+          if (sub == c) a = acc[c];
+        const int64_t off = row * ld + c0 + sub;
+        double r = fma(diag, static_cast<double>(x[off]), a);
+        r *= ep.alpha;
+        if (ep.z1) r = fma(ep.beta, static_cast<double>(ep.z1[off]), r);
+        if (ep.z2) r = fma(ep.gamma, static_cast<double>(ep.z2[off]), r);
+        if (ep.z3) r = fma(ep.delta, static_cast<double>(ep.z3[off]), r);
+        y[off] = static_cast<XT>(r);
+      }
+    }
+  }
+}
+
+template <class VT, class XT, int LD, int G>
+void launch_vec(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
+                const int* stop) {
+  const int threads = 256;
+  const int64_t need = (op.n * G + threads - 1) / threads;
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(ex.sms) * 8)));
+  k_spmm_vec<VT, XT, LD, G><<<grid, threads, 0, ex.stream>>>(op.n, op.indptr, op.indices, vals, op.diag, x, y,
+                                                              ep, stop);
+  SI_LAUNCH_CHECK();
+}
+
+template <class VT, class XT, int G>
+void launch_generic(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, int ld, int k,
+                    const Epilogue<XT>& ep, const int* stop) {
+  const int threads = 256;
+  const int64_t need = (op.n * G + threads - 1) / threads;
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(ex.sms) * 8)));
+  k_spmm_generic<VT, XT, G><<<grid, threads, 0, ex.stream>>>(op.n, op.indptr, op.indices, vals, op.diag, x, y,
+                                                              ld, k, ep, stop);
+  SI_LAUNCH_CHECK();
+}
+
+template <class VT, class XT, int LD>
+void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
+                const int* stop) {
+  switch (spmm_group_lanes(op)) {
+    case 4: launch_vec<VT, XT, LD, 4>(ex, op, vals, x, y, ep, stop); break;
+    case 8: launch_vec<VT, XT, LD, 8>(ex, op, vals, x, y, ep, stop); break;
+    case 16: launch_vec<VT, XT, LD, 16>(ex, op, vals, x, y, ep, stop); break;
+    default: launch_vec<VT, XT, LD, 32>(ex, op, vals, x, y, ep, stop); break;
+  }
+}
+
+template <class VT, class XT>
+void dispatch(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, int ld, int k,
+              const Epilogue<XT>& ep, const int* stop) {
+  // vector gathers need the row start aligned to the vector width (32 B for
+  // f64 and for 8-wide f32, 16 B for 4-wide f32); otherwise use the generic path
+  const uintptr_t a = reinterpret_cast<uintptr_t>(x);
+  const bool aligned = (sizeof(XT) == 4 && ld == 4) ? (a % 16 == 0) : (a % 32 == 0);
+  if (aligned && ld == 4) return dispatch_g<VT, XT, 4>(ex, op, vals, x, y, ep, stop);
+  if (aligned && ld == 8) return dispatch_g<VT, XT, 8>(ex, op, vals, x, y, ep, stop);
+  if (aligned && ld == 16) return dispatch_g<VT, XT, 16>(ex, op, vals, x, y, ep, stop);
+  switch (spmm_group_lanes(op)) {
+    case 4: return launch_generic<VT, XT, 4>(ex, op, vals, x, y, ld, k, ep, stop);
+    case 8: return launch_generic<VT, XT, 8>(ex, op, vals, x, y, ld, k, ep, stop);
+    case 16: return launch_generic<VT, XT, 16>(ex, op, vals, x, y, ld, k, ep, stop);
+    default: return launch_generic<VT, XT, 32>(ex, op, vals, x, y, ld, k, ep, stop);
+  }
+}
+
+}  // namespace
+
+int spmm_group_lanes(const OpDev& op) {
+  const double mean = op.n > 0 ? static_cast<double>(op.nnz) / static_cast<double>(op.n) : 0.0;
+  if (mean <= 6.0) return 4;
+  if (mean <= 20.0) return 8;
+  if (mean <= 56.0) return 16;
+  return 32;
+}
+
+template <class XT>
+void spmm_dev(const Exec& ex, const OpDev& op, const XT* x, XT* y, int ld, int k, const Epilogue<XT>& ep,
+              const int* stop, bool use_f32_values) {
+  if (op.n == 0) return;
+  SI_REQUIRE(k >= 1 && k <= ld, SI_INVALID_ARGUMENT, "spmm: need 1 <= k <= ld");
+  SI_REQUIRE(x != y, SI_INVALID_ARGUMENT, "spmm: x and y must not alias");
+  if (use_f32_values) {
+    SI_REQUIRE(op.v32 != nullptr, SI_INVALID_ARGUMENT, "spmm: f32 values requested but absent");
+    dispatch<float, XT>(ex, op, op.v32, x, y, ld, k, ep, stop);
+  } else {
+    SI_REQUIRE(op.v64 != nullptr, SI_INVALID_ARGUMENT, "spmm: f64 values absent");
+    dispatch<double, XT>(ex, op, op.v64, x, y, ld, k, ep, stop);
+  }
+}
+
+template void spmm_dev<double>(const Exec&, const OpDev&, const double*, double*, int, int,
+                               const Epilogue<double>&, const int*, bool);
+template void spmm_dev<float>(const Exec&, const OpDev&, const float*, float*, int, int,
+                              const Epilogue<float>&, const int*, bool);
+
+}  // namespace si

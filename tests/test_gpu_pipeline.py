@@ -1,0 +1,149 @@
+"""spectral_init end to end through the C ABI (tests/integration/
+test_e2e_validation.rs and src/lib.rs:295-375 of the reference)."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import CONNECTED, load_csr, load_graph, load_npz
+from oracle import spectral_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def path4():
+    return sp.csr_matrix((np.ones(6, np.float32), np.array([1, 0, 2, 1, 3, 2]), np.array([0, 1, 3, 5, 6])),
+                         shape=(4, 4))
+
+
+@pytest.mark.parametrize("ds", CONNECTED)
+def test_e2e_residual_quality(gpu_ctx, ds):
+    import spectral_init_b200 as si
+    g = load_graph(ds)
+    out = si.spectral_init(g, 2, 42, ctx=gpu_ctx)
+    assert out.shape == (g.shape[0], 2) and out.dtype == np.float32 and np.all(np.isfinite(out))
+    expansion = float(load_npz(ds, "comp_f_scaling.npz")["expansion"])
+    lap = load_csr(ds, "comp_b_laplacian.npz")
+    ref = load_npz(ds, "comp_d_eigensolver.npz")["eigenvalues"]
+    des = out.astype(np.float64) / expansion
+    for c in range(2):
+        assert O.eigenpair_residual(lap, des[:, c], ref[c + 1]) < 0.005
+
+
+@pytest.mark.parametrize("ds", ["circles_300", "near_dupes_100"])
+def test_e2e_subspace(gpu_ctx, ds):
+    import spectral_init_b200 as si
+    out = si.spectral_init(load_graph(ds), 2, 42, ctx=gpu_ctx).astype(np.float64)
+    ref = load_npz(ds, "comp_d_eigensolver.npz")["eigenvectors"][:, 1:3]
+    assert O.subspace_gram_det_kd(out, ref) > 0.95
+
+
+@pytest.mark.parametrize("ds", CONNECTED)
+def test_e2e_matches_oracle_prenoise_up_to_sign(gpu_ctx, ds):
+    """Final scaled embedding vs the oracle's pre-noise embedding, per-axis sign
+    free; tolerance = noise (1e-4 sigma, 6 sigma) + solver error."""
+    import spectral_init_b200 as si
+    g = load_graph(ds)
+    out = si.spectral_init(g, 2, 42, ctx=gpu_ctx).astype(np.float64)
+    pre = O.spectral_init_prenoise(g, 2, 42)
+    ref = O.scale_coords(pre, 10.0).astype(np.float64)
+    evals = load_npz(ds, "comp_d_eigensolver.npz")["eigenvalues"]
+    for c in range(2):
+        err = min(np.max(np.abs(out[:, c] - ref[:, c])), np.max(np.abs(out[:, c] + ref[:, c])))
+        assert err < 2e-3, (ds, c, err, evals)
+
+
+@pytest.mark.parametrize("ds", ["blobs_50", "moons_200", "circles_300", "blobs_connected_200", "near_dupes_100"])
+def test_e2e_exact_knn_graphs(gpu_ctx, ds):
+    import spectral_init_b200 as si
+    g = load_graph(ds, exact=True)
+    out = si.spectral_init(g, 2, 42, ctx=gpu_ctx)
+    assert out.shape == (g.shape[0], 2) and np.all(np.isfinite(out))
+
+
+def test_e2e_disconnected_component_separation(gpu_ctx):
+    import spectral_init_b200 as si
+    g = load_graph("disconnected_200")
+    out = si.spectral_init(g, 2, 42, ctx=gpu_ctx).astype(np.float64)
+    labels = load_npz("disconnected_200", "comp_c_components.npz")["labels"]
+    cents = np.array([out[labels == c].mean(axis=0) for c in np.unique(labels)])
+    d = np.sqrt(((cents[:, None] - cents[None]) ** 2).sum(-1))
+    assert d[np.triu_indices(len(cents), 1)].min() > 1.0
+
+
+@pytest.mark.parametrize("ds", ["blobs_50", "blobs_500", "blobs_5000", "disconnected_200"])
+def test_e2e_disconnected_matches_oracle(gpu_ctx, ds):
+    import spectral_init_b200 as si
+    g = load_graph(ds)
+    out = si.spectral_init(g, 2, 42, ctx=gpu_ctx).astype(np.float64)
+    pre = O.spectral_init_prenoise(g, 2, 42)
+    ref = O.scale_coords(pre, 10.0).astype(np.float64)
+    # each component is an independent eigenproblem: compare per component up to sign
+    labels, nc = O.find_components(g)
+    assert nc > 1
+    for c in range(nc):
+        m = labels == c
+        for d in range(2):
+            a, b = out[m, d], ref[m, d]
+            ca = a - a.mean()
+            cb = b - b.mean()
+            assert abs(a.mean() - b.mean()) < 1e-2 or np.max(np.abs(a - b)) < 1e-2
+            if np.linalg.norm(cb) > 1e-3:
+                cos = abs(ca @ cb) / (np.linalg.norm(ca) * np.linalg.norm(cb))
+                assert cos > 0.99, (ds, c, d, cos)
+
+
+def test_disconnected_many_components_needs_data(gpu_ctx):
+    import spectral_init_b200 as si
+    from oracle import graphgen
+    parts = [graphgen.ring_graph(30 + 3 * i, 2) for i in range(6)]
+    g = graphgen.block_diagonal(parts)
+    with pytest.raises(si.InvalidGraph):
+        si.spectral_init(g, 2, 42, ctx=gpu_ctx)
+    rng = np.random.default_rng(0)
+    data = np.concatenate([rng.normal(5 * i, 1.0, size=(p.shape[0], 3)) for i, p in enumerate(parts)]).astype(np.float32)
+    out = si.spectral_init(g, 2, 42, data=data, ctx=gpu_ctx)
+    ref = O.scale_coords(O.spectral_init_prenoise(g, 2, 42, data=data), 10.0)
+    assert out.shape == (g.shape[0], 2) and np.all(np.isfinite(out))
+    # meta-embedding places components the same way up to per-axis sign
+    labels, nc = O.find_components(g)
+    for d in range(2):
+        cg = np.array([out[labels == c, d].mean() for c in range(nc)])
+        cr = np.array([ref[labels == c, d].mean() for c in range(nc)])
+        assert min(np.max(np.abs(cg - cr)), np.max(np.abs(cg + cr))) < 1e-2
+
+
+def test_output_sign_convention_and_shape(gpu_ctx):
+    import spectral_init_b200 as si
+    out = si.spectral_init(path4(), 2, 42, ctx=gpu_ctx)
+    assert out.shape == (4, 2)
+    for c in range(2):
+        assert out[np.argmax(np.abs(out[:, c])), c] > 0
+
+
+def test_python_compat_and_rust_native_same_subspace(gpu_ctx):
+    import spectral_init_b200 as si
+    r1 = si.spectral_init(path4(), 2, 42, ctx=gpu_ctx)
+    r2 = si.spectral_init(path4(), 2, 42, si.SpectralInitConfig(compute_mode=si.ComputeMode.RustNative), ctx=gpu_ctx)
+    for c in range(2):
+        cos = abs(r1[:, c] @ r2[:, c]) / (np.linalg.norm(r1[:, c]) * np.linalg.norm(r2[:, c]))
+        assert cos > 0.999
+
+
+def test_errors(gpu_ctx):
+    import spectral_init_b200 as si
+    with pytest.raises(si.InvalidGraph):
+        si.spectral_init(path4(), 0, 42, ctx=gpu_ctx)
+    with pytest.raises(si.InvalidGraph):
+        si.spectral_init(sp.csr_matrix((0, 0), dtype=np.float32), 2, 42, ctx=gpu_ctx)
+    two = sp.csr_matrix((np.ones(2, np.float32), np.array([1, 0]), np.array([0, 1, 2])), shape=(2, 2))
+    with pytest.raises(si.TooFewNodes) as ei:
+        si.spectral_init(two, 3, 42, ctx=gpu_ctx)
+    assert ei.value.n == 2 and ei.value.dims == 3
+
+
+def test_deterministic_for_a_seed(gpu_ctx):
+    import spectral_init_b200 as si
+    g = load_graph("blobs_connected_2000")
+    a = si.spectral_init(g, 2, 7, ctx=gpu_ctx)
+    b = si.spectral_init(g, 2, 7, ctx=gpu_ctx)
+    assert np.array_equal(a, b)
