@@ -129,6 +129,9 @@ typedef struct si_ctx si_ctx;
 /* ---- context -------------------------------------------------------------- */
 void si_config_default(si_config* cfg);
 int32_t si_abi_version(void);
+/* Number of CUDA kernels this library has launched in this process
+ * (diagnostics; no counterpart in the crate). */
+uint64_t si_kernel_launches(void);
 si_status si_ctx_create(int32_t device, si_ctx** out);
 void si_ctx_destroy(si_ctx* ctx);
 const char* si_last_error(const si_ctx* ctx);

@@ -141,8 +141,9 @@ def smooth_knn_dist(dists: np.ndarray, k: float, n_iter: int = 64, local_connect
 def membership_strengths(knn_i: np.ndarray, knn_d: np.ndarray, sigma: np.ndarray, rho: np.ndarray, n: int):
     d = knn_d.astype(np.float32)
     diff = d - rho[:, None]
+    safe_sigma = np.where(sigma == 0.0, np.float32(1.0), sigma)[:, None]
     val = np.where((diff <= 0.0) | (sigma[:, None] == 0.0), np.float32(1.0),
-                   np.exp(-diff / sigma[:, None])).astype(np.float32)
+                   np.exp(-np.maximum(diff, 0.0) / safe_sigma)).astype(np.float32)
     rows = np.repeat(np.arange(n), knn_i.shape[1])
     cols = knn_i.reshape(-1)
     v = val.reshape(-1)

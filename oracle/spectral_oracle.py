@@ -297,7 +297,10 @@ def _sorted_eig(a, b, size, largest):
     return w[idx], v[:, idx]
 
 
-def lobpcg_core(apply, x: np.ndarray, tol: float, maxiter: int, largest: bool = False) -> LobpcgResult:
+def lobpcg_core(apply, x: np.ndarray, tol: float, maxiter: int, largest: bool = False,
+                callback=None) -> LobpcgResult:
+    """``callback(iteration, residual_norms)`` may return True to stop early
+    (treated like reaching ``maxiter``)."""
     n, size_x = x.shape
     try:
         x, _ = _ortho(x)
@@ -325,6 +328,8 @@ def lobpcg_core(apply, x: np.ndarray, tol: float, maxiter: int, largest: bool = 
             converged = True
             break
         if it >= maxiter:
+            break
+        if callback is not None and callback(it, rn):
             break
         it += 1
         ra = r[:, active]

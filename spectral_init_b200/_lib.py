@@ -63,6 +63,7 @@ vp = C.c_void_p
 _SIGNATURES = {
     "si_config_default": (None, [C.POINTER(SiConfig)]),
     "si_abi_version": (C.c_int32, []),
+    "si_kernel_launches": (C.c_uint64, []),
     "si_ctx_create": (C.c_int, [C.c_int32, C.POINTER(vp)]),
     "si_ctx_destroy": (None, [vp]),
     "si_last_error": (C.c_char_p, [vp]),

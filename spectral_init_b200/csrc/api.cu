@@ -10,6 +10,8 @@
 
 #include "pipeline.h"
 
+std::atomic<uint64_t> si::g_kernel_launches{0};
+
 struct si_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -161,6 +163,8 @@ void si_config_default(si_config* cfg) {
 }
 
 int32_t si_abi_version(void) { return SI_ABI_VERSION; }
+
+uint64_t si_kernel_launches(void) { return si::g_kernel_launches.load(std::memory_order_relaxed); }
 
 si_status si_ctx_create(int32_t device, si_ctx** out) {
   if (out == nullptr) return SI_INVALID_ARGUMENT;

@@ -105,22 +105,28 @@ __global__ void __launch_bounds__(GT) k_gram(GramParams<XT> p) {
     }
     __syncthreads();
   }
+  // partials entry-major: the finishing CTA reads each entry's partials coalesced
 #pragma unroll
   for (int q = 0; q < GEPT; ++q)
-    if (q < cnt) p.partial[static_cast<int64_t>(blockIdx.x) * p.ne + tid + q * GT] = acc[q];
+    if (q < cnt) p.partial[static_cast<int64_t>(tid + q * GT) * gridDim.x + blockIdx.x] = acc[q];
   __threadfence();
   __syncthreads();
   if (tid == 0) last = (atomicAdd(p.counter, 1u) == gridDim.x - 1);
   __syncthreads();
   if (!last) return;
   __threadfence();
-  for (int e = tid; e < p.ne; e += GT) {
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int e = warp; e < p.ne; e += GT / 32) {
+    const double* pe = p.partial + static_cast<int64_t>(e) * gridDim.x;
     double s = 0.0;
-    for (int c = 0; c < static_cast<int>(gridDim.x); ++c) s += p.partial[static_cast<int64_t>(c) * p.ne + e];
-    int a, b, o1, o2;
-    gram_entry(p.mode, p.P, p.Q, e, a, b, o1, o2);
-    p.out[o1] = s;
-    if (o2 >= 0) p.out[o2] = s;
+    for (int c = lane; c < static_cast<int>(gridDim.x); c += 32) s += pe[c];
+    s = warp_sum(s);
+    if (lane == 0) {
+      int a, b, o1, o2;
+      gram_entry(p.mode, p.P, p.Q, e, a, b, o1, o2);
+      p.out[o1] = s;
+      if (o2 >= 0) p.out[o2] = s;
+    }
   }
   if (tid == 0) *p.counter = 0u;
 }
@@ -196,7 +202,7 @@ __global__ void k_colnorms(const XT* a, const XT* b, const double* lam, int m, i
   if (threadIdx.x < m) {
     double s = 0.0;
     for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += red[w][threadIdx.x];
-    partial[static_cast<int64_t>(blockIdx.x) * MAXM + threadIdx.x] = s;
+    partial[static_cast<int64_t>(threadIdx.x) * gridDim.x + blockIdx.x] = s;
   }
   __threadfence();
   __syncthreads();
@@ -204,10 +210,11 @@ __global__ void k_colnorms(const XT* a, const XT* b, const double* lam, int m, i
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (threadIdx.x < m) {
+  for (int c = warp; c < m; c += blockDim.x >> 5) {
     double s = 0.0;
-    for (int c = 0; c < static_cast<int>(gridDim.x); ++c) s += partial[static_cast<int64_t>(c) * MAXM + threadIdx.x];
-    out[threadIdx.x] = sqrt(s);
+    for (int b = lane; b < static_cast<int>(gridDim.x); b += 32) s += partial[static_cast<int64_t>(c) * gridDim.x + b];
+    s = warp_sum(s);
+    if (lane == 0) out[c] = sqrt(s);
   }
   if (threadIdx.x == 0) *counter = 0u;
 }
@@ -247,11 +254,14 @@ __global__ void k_sumsq(const double* v, int64_t n, double* partial, unsigned* c
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     double s = 0.0;
-    for (int c = 0; c < static_cast<int>(gridDim.x); ++c) s += partial[c];
-    *out = s;
-    *counter = 0u;
+    for (int c = threadIdx.x; c < static_cast<int>(gridDim.x); c += 32) s += partial[c];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) {
+      *out = s;
+      *counter = 0u;
+    }
   }
 }
 
@@ -390,11 +400,14 @@ __global__ void k_maxabs(const double* x, int64_t n, int k, int ld, double* part
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     double s = 0.0;
-    for (int c = 0; c < static_cast<int>(gridDim.x); ++c) s = fmax(s, partial[c]);
-    *out = s;
-    *counter = 0u;
+    for (int c = threadIdx.x; c < static_cast<int>(gridDim.x); c += 32) s = fmax(s, partial[c]);
+    s = warp_max(s);
+    if (threadIdx.x == 0) {
+      *out = s;
+      *counter = 0u;
+    }
   }
 }
 
@@ -636,7 +649,7 @@ int grid_rows(const Exec& ex, int64_t items, int threads = 256, int per_sm = 8) 
 template <class XT>
 void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, int ns, int nblk, int m, int ld,
               int64_t n, double* out, const int* stop) {
-  SI_REQUIRE(nblk <= 8 && m <= MAXM && nblk * m <= GMAXW, SI_INVALID_ARGUMENT, "gram: too many columns");
+  SI_REQUIRE(nblk >= 1 && nblk <= 8 && m >= 1 && nblk * m <= GMAXW, SI_INVALID_ARGUMENT, "gram: too many columns");
   GramParams<XT> p{};
   for (int b = 0; b < nblk; ++b) p.blk[b] = blk[b];
   p.nblk = nblk;

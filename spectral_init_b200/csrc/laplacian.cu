@@ -221,8 +221,8 @@ void validate_graph(const Exec& ex, const GraphDev& g) {
   SI_REQUIRE(g.n >= 0 && g.nnz >= 0, SI_INVALID_GRAPH, "invalid graph: negative size");
   SI_REQUIRE(g.n < (int64_t(1) << 32), SI_INVALID_GRAPH, "invalid graph: more than 2^32-1 rows");
   SI_REQUIRE(g.indptr != nullptr, SI_INVALID_ARGUMENT, "graph indptr is null");
-  SI_REQUIRE(g.nnz == 0 || (g.indices != nullptr && g.data != nullptr), SI_INVALID_ARGUMENT,
-             "graph indices/data are null");
+  // data may be null for structure-only validation (f64 matrices carry their own values)
+  SI_REQUIRE(g.nnz == 0 || g.indices != nullptr, SI_INVALID_ARGUMENT, "graph indices are null");
   DevBuf<unsigned> err(1, ex.stream);
   err.zero();
   k_validate<<<grid_for(ex, std::max<int64_t>(g.n, 1)), 256, 0, ex.stream>>>(g.n, g.nnz, g.indptr, g.indices,

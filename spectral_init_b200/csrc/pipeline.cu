@@ -66,6 +66,13 @@ __global__ void k_perm_fill(int64_t n, const uint32_t* __restrict__ perm, const 
   }
 }
 
+// dst[i] = src[i] - base for i <= n (component-relative row pointers)
+__global__ void k_rebase(int64_t n, const uint64_t* __restrict__ src, uint64_t base, uint64_t* __restrict__ dst) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i <= n; i += stride)
+    dst[i] = src[i] - base;
+}
+
 __global__ void k_label_counts(int64_t n, const uint32_t* __restrict__ labels, uint64_t* __restrict__ counts) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
@@ -333,12 +340,18 @@ void embed_disconnected_dev(const Exec& ex, const GraphDev& g, const uint32_t* l
       SI_CUDA(cudaStreamSynchronize(ex.stream));
       continue;
     }
+    // component view: its rows are contiguous in the permuted CSR; every array
+    // handed to the solver is component-relative (indptr rebased to 0)
+    const uint64_t ebase = h_pptr[off];
+    DevBuf<uint64_t> sub_ptr(sz + 1, ex.stream);
+    k_rebase<<<grid_for(ex, sz + 1), 256, 0, ex.stream>>>(sz, pptr.get() + off, ebase, sub_ptr.get());
+    SI_LAUNCH_CHECK();
     GraphDev sub;
     sub.n = sz;
-    sub.nnz = static_cast<int64_t>(h_pptr[off + sz] - h_pptr[off]);
-    sub.indptr = pptr.get() + off;
-    sub.indices = pidx.get();
-    sub.data = pval.get();
+    sub.nnz = static_cast<int64_t>(h_pptr[off + sz] - ebase);
+    sub.indptr = sub_ptr.get();
+    sub.indices = pidx.get() + ebase;
+    sub.data = pval.get() + ebase;
     DevBuf<double> coords;
     SolverStats cst;
     std::vector<double> ev;

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -32,7 +33,14 @@ struct Error : std::runtime_error {
                             __FILE__ + ":" + std::to_string(__LINE__) + ")");           \
   } while (0)
 
-#define SI_LAUNCH_CHECK() SI_CUDA(cudaGetLastError())
+// Kernels launched by this library in this process (diagnostics export).
+extern std::atomic<uint64_t> g_kernel_launches;
+
+#define SI_LAUNCH_CHECK()                                            \
+  do {                                                               \
+    ::si::g_kernel_launches.fetch_add(1, std::memory_order_relaxed); \
+    SI_CUDA(cudaGetLastError());                                     \
+  } while (0)
 
 #define SI_REQUIRE(cond, code, msg)            \
   do {                                         \

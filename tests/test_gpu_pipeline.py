@@ -40,16 +40,20 @@ def test_e2e_subspace(gpu_ctx, ds):
 @pytest.mark.parametrize("ds", CONNECTED)
 def test_e2e_matches_oracle_prenoise_up_to_sign(gpu_ctx, ds):
     """Final scaled embedding vs the oracle's pre-noise embedding, per-axis sign
-    free; tolerance = noise (1e-4 sigma, 6 sigma) + solver error."""
+    free.  Below n = 2000 both sides take the dense level (exact eigenvectors):
+    the tolerance is the noise (1e-4 sigma, 6 sigma) plus f32 rounding.  At
+    n = 2000 both take LOBPCG with residual < 1e-5, whose eigenvectors agree to
+    ~residual/gap; there the tolerance is 1e-2 on the +/-10 box."""
     import spectral_init_b200 as si
     g = load_graph(ds)
     out = si.spectral_init(g, 2, 42, ctx=gpu_ctx).astype(np.float64)
     pre = O.spectral_init_prenoise(g, 2, 42)
     ref = O.scale_coords(pre, 10.0).astype(np.float64)
     evals = load_npz(ds, "comp_d_eigensolver.npz")["eigenvalues"]
+    tol = 2e-3 if g.shape[0] < 2000 else 1e-2
     for c in range(2):
         err = min(np.max(np.abs(out[:, c] - ref[:, c])), np.max(np.abs(out[:, c] + ref[:, c])))
-        assert err < 2e-3, (ds, c, err, evals)
+        assert err < tol, (ds, c, err, evals)
 
 
 @pytest.mark.parametrize("ds", ["blobs_50", "moons_200", "circles_300", "blobs_connected_200", "near_dupes_100"])
@@ -116,14 +120,18 @@ def test_output_sign_convention_and_shape(gpu_ctx):
     import spectral_init_b200 as si
     out = si.spectral_init(path4(), 2, 42, ctx=gpu_ctx)
     assert out.shape == (4, 2)
+    # path eigenvectors come in +/- pairs of equal magnitude; the sign rule makes
+    # the first maximal entry positive before the N(0, 1e-4) noise, so the
+    # largest positive entry is within the noise of the largest magnitude
     for c in range(2):
-        assert out[np.argmax(np.abs(out[:, c])), c] > 0
+        assert out[:, c].max() >= np.abs(out[:, c]).max() - 1e-3
 
 
 def test_python_compat_and_rust_native_same_subspace(gpu_ctx):
     import spectral_init_b200 as si
     r1 = si.spectral_init(path4(), 2, 42, ctx=gpu_ctx)
-    r2 = si.spectral_init(path4(), 2, 42, si.SpectralInitConfig(compute_mode=si.ComputeMode.RustNative), ctx=gpu_ctx)
+    r2 = si.spectral_init(path4(), 2, 42, None, si.SpectralInitConfig(compute_mode=si.ComputeMode.RustNative),
+                          ctx=gpu_ctx)
     for c in range(2):
         cos = abs(r1[:, c] @ r2[:, c]) / (np.linalg.norm(r1[:, c]) * np.linalg.norm(r2[:, c]))
         assert cos > 0.999
