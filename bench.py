@@ -56,6 +56,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--spmm-profile", action="store_true", help="SpMM launches only (n=--n), for ncu")
+    p.add_argument("--spmm-prec", choices=["both", "f64", "f32"], default="both",
+                   help="with --spmm-profile: which SpMM precision to run")
     p.add_argument("--profile-solve", action="store_true",
                    help="one FP64 and one mixed eigensolve only (after one warm-up each), for ncu launch lists")
     return p.parse_args()
@@ -233,8 +235,10 @@ def run_ours(a):
     x32 = x64.float()
     y32 = torch.empty_like(x32)
     torch.cuda.synchronize()
-    ms64 = time_spmm(x64, y64, False, a.spmm_reps)
-    ms32 = time_spmm(x32, y32, True, a.spmm_reps)
+    run64 = not (a.spmm_profile and a.spmm_prec == "f32")
+    run32 = not (a.spmm_profile and a.spmm_prec == "f64")
+    ms64 = time_spmm(x64, y64, False, a.spmm_reps) if run64 else float("nan")
+    ms32 = time_spmm(x32, y32, True, a.spmm_reps) if run32 else float("nan")
     bytes64 = nnz * (4 + 8) + (n + 1) * 8 + 2 * n * 4 * 8
     bytes32 = nnz * (4 + 4) + (n + 1) * 8 + 2 * n * 4 * 4
     gbs64 = bytes64 / (ms64 * 1e-3) / 1e9

@@ -132,6 +132,221 @@ __global__ void __launch_bounds__(GT) k_gram(GramParams<XT> p) {
 }
 
 // ---------------------------------------------------------------------------
+// Gram of one LOBPCG iteration for 4-column blocks:
+//   G = S^T [S AS],  S = [X R P], AS = [AX AR AP]  (12 x 24).
+// Rows stream through shared memory in 64-row tiles with cp.async double
+// buffering; each lane owns a 3 x 3 register tile of G (lane = 8 * a + b:
+// S columns 3a..3a+2 against T columns 3b..3b+2), so a warp covers all 288
+// entries of a row with six shared loads per lane.  Accumulation is f64 (the
+// product of two f32 values is exact in f64).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+constexpr int G4_TR = 64;
+
+template <class XT>
+__global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const XT* __restrict__ R,
+                                               const XT* __restrict__ P, const XT* __restrict__ AX,
+                                               const XT* __restrict__ AR, const XT* __restrict__ AP, int64_t n,
+                                               double* partial, double* out, unsigned* counter,
+                                               const int* __restrict__ stop) {
+  if (stop != nullptr && *stop != 0) return;
+  __shared__ __align__(16) XT tile[2][G4_TR][24];
+  __shared__ double red[8][288];
+  __shared__ bool last;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ai = 3 * (lane >> 3);  // S column base
+  const int bj = 3 * (lane & 7);   // T column base
+  double acc[3][3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) acc[p][q] = 0.0;
+  const XT* src[6] = {X, R, P, AX, AR, AP};
+  constexpr int EPC = 16 / sizeof(XT);          // elements per 16-byte chunk
+  constexpr int CPB = 4 / EPC;                  // chunks per (row, block)
+  constexpr int NCH = G4_TR * 6 * CPB;
+  const int64_t ntiles = (n + G4_TR - 1) / G4_TR;
+  auto load_tile = [&](int64_t t, int buf) {
+    const int64_t row0 = t * G4_TR;
+    for (int c = tid; c < NCH; c += 256) {
+      const int b = c / (G4_TR * CPB);
+      const int rem = c % (G4_TR * CPB);
+      const int r = rem / CPB, h = rem % CPB;
+      const int64_t row = row0 + r;
+      const bool ok = row < n;
+      cp_async16(&tile[buf][r][b * 4 + h * EPC], src[b] + (ok ? row : 0) * 4 + h * EPC, ok ? 16 : 0);
+    }
+    cp_async_commit();
+  };
+  int64_t t = blockIdx.x;
+  int buf = 0;
+  if (t < ntiles) load_tile(t, 0);
+  for (; t < ntiles; t += gridDim.x) {
+    const int64_t tn = t + gridDim.x;
+    if (tn < ntiles) {
+      load_tile(tn, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int r = warp; r < G4_TR; r += 8) {
+      const XT* row = tile[buf][r];
+      const double s0 = static_cast<double>(row[ai]), s1 = static_cast<double>(row[ai + 1]),
+                   s2 = static_cast<double>(row[ai + 2]);
+      const double t0 = static_cast<double>(row[bj]), t1 = static_cast<double>(row[bj + 1]),
+                   t2 = static_cast<double>(row[bj + 2]);
+      acc[0][0] = fma(s0, t0, acc[0][0]);
+      acc[0][1] = fma(s0, t1, acc[0][1]);
+      acc[0][2] = fma(s0, t2, acc[0][2]);
+      acc[1][0] = fma(s1, t0, acc[1][0]);
+      acc[1][1] = fma(s1, t1, acc[1][1]);
+      acc[1][2] = fma(s1, t2, acc[1][2]);
+      acc[2][0] = fma(s2, t0, acc[2][0]);
+      acc[2][1] = fma(s2, t1, acc[2][1]);
+      acc[2][2] = fma(s2, t2, acc[2][2]);
+    }
+    __syncthreads();
+    buf ^= 1;
+  }
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) red[warp][(ai + p) * 24 + bj + q] = acc[p][q];
+  __syncthreads();
+  const int G = gridDim.x;
+  for (int e = tid; e < 288; e += 256) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) s += red[w][e];
+    partial[static_cast<int64_t>(e) * G + blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(counter, 1u) == static_cast<unsigned>(G) - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // finishing CTA: four entries per warp pass so a lane keeps many loads in flight
+  for (int e0 = warp * 4; e0 < 288; e0 += 32) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int c = lane; c < G; c += 32) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) s[q] += partial[static_cast<int64_t>(e0 + q) * G + c];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double v = warp_sum(s[q]);
+      const int e = e0 + q;
+      const int i = e / 24, j = e % 24;
+      if (lane == 0) {
+        if (j < 12) {
+          if (i <= j) {
+            out[i * 12 + j] = v;
+            out[j * 12 + i] = v;
+          }
+        } else {
+          const int jj = j - 12;
+          if (i <= jj) {
+            out[144 + i * 12 + jj] = v;
+            out[144 + jj * 12 + i] = v;
+          }
+        }
+      }
+    }
+  }
+  if (tid == 0) *counter = 0u;
+}
+
+// LOBPCG update with 4-column blocks: four threads per row, thread j produces
+// output column j (inputs are read as 4-vectors; the four threads of a row
+// share the same sectors).
+template <class XT>
+__global__ void __launch_bounds__(256) k_lobpcg_update4(LobpcgBlocks<XT> b, const LobpcgCtrl* __restrict__ ctrl,
+                                                        int64_t n, int init_mode) {
+  __shared__ double sC[3][4][4];
+  __shared__ double sLam[4];
+  __shared__ int sF[4];
+  if (threadIdx.x == 0) {
+    sF[0] = ctrl->done;
+    sF[1] = ctrl->copy_best;
+    sF[2] = ctrl->has_p;
+    sF[3] = ctrl->m;
+  }
+  if (threadIdx.x < 48) {
+    const int w = threadIdx.x / 16, r = (threadIdx.x / 4) % 4, c = threadIdx.x % 4;
+    const double* src = w == 0 ? ctrl->Cx : (w == 1 ? ctrl->Cr : ctrl->Cp);
+    sC[w][r][c] = src[r * MAXM + c];
+  }
+  if (threadIdx.x < 4) sLam[threadIdx.x] = ctrl->lam[threadIdx.x];
+  __syncthreads();
+  const int done = sF[0], copy_best = sF[1], use_p = sF[2], m = sF[3];
+  if (done && !copy_best) return;
+  const int64_t total = n * 4;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;  // multiple of 32
+  // the loop condition uses the warp's base index, so all lanes of a warp run
+  // the same trip count and reach the __syncwarp below together
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; (t & ~int64_t(31)) < total;
+       t += stride) {
+    const bool valid = t < total;  // rows are 4-aligned: a row's lanes agree
+    const int64_t i = valid ? (t >> 2) : 0;
+    const int j = static_cast<int>(t & 3);
+    const int64_t o = i * 4;
+    if (valid && copy_best) b.Xbest[o + j] = b.X[o + j];
+    if (done) continue;  // uniform
+    // lanes past the end compute on row 0 (always readable) and store nothing
+    double x[4], ax[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      x[c] = static_cast<double>(b.X[o + c]);
+      ax[c] = static_cast<double>(b.AX[o + c]);
+    }
+    double pn = 0.0, apn = 0.0;
+    if (!init_mode) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        pn = fma(static_cast<double>(b.R[o + c]), sC[1][c][j], pn);
+        apn = fma(static_cast<double>(b.AR[o + c]), sC[1][c][j], apn);
+      }
+      if (use_p) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          pn = fma(static_cast<double>(b.P[o + c]), sC[2][c][j], pn);
+          apn = fma(static_cast<double>(b.AP[o + c]), sC[2][c][j], apn);
+        }
+      }
+    }
+    double xn = pn, axn = apn;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      xn = fma(x[c], sC[0][c][j], xn);
+      axn = fma(ax[c], sC[0][c][j], axn);
+    }
+    // every thread of the row has read its inputs before any column is overwritten
+    __syncwarp();
+    if (!valid) continue;
+    const bool active = j < m;
+    const XT xs = static_cast<XT>(active ? xn : 0.0);
+    const XT axs = static_cast<XT>(active ? axn : 0.0);
+    b.X[o + j] = xs;
+    b.AX[o + j] = axs;
+    b.R[o + j] = static_cast<XT>(active ? static_cast<double>(axs) - sLam[j] * static_cast<double>(xs) : 0.0);
+    if (!init_mode) {
+      b.P[o + j] = static_cast<XT>(active ? pn : 0.0);
+      b.AP[o + j] = static_cast<XT>(active ? apn : 0.0);
+    }
+  }
+}
+
 template <class XT>
 __global__ void k_combine(const XT* in0, const XT* in1, const XT* in2, const double* c0, const double* c1,
                           const double* c2, int nin, XT* out, int m_in, int m_out, int cstride, int ld,
@@ -650,6 +865,16 @@ template <class XT>
 void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, int ns, int nblk, int m, int ld,
               int64_t n, double* out, const int* stop) {
   SI_REQUIRE(nblk >= 1 && nblk <= 8 && m >= 1 && nblk * m <= GMAXW, SI_INVALID_ARGUMENT, "gram: too many columns");
+  if (mode == GRAM_SYM2 && ns == 3 && nblk == 6 && m == 4 && ld == 4) {
+    // the per-iteration LOBPCG Gram of 4-column blocks
+    const int64_t ntiles = (n + G4_TR - 1) / G4_TR;
+    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ex.sms) * 2)));
+    w.ensure(static_cast<size_t>(grid) * 288, ex.stream);
+    k_gram4<XT><<<grid, 256, 0, ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4], blk[5], n, w.partial.get(), out,
+                                            w.counter.get(), stop);
+    SI_LAUNCH_CHECK();
+    return;
+  }
   GramParams<XT> p{};
   for (int b = 0; b < nblk; ++b) p.blk[b] = blk[b];
   p.nblk = nblk;
@@ -790,7 +1015,7 @@ void lobpcg_update_dev(const Exec& ex, const LobpcgBlocks<XT>& b, const LobpcgCt
   if (n == 0) return;
   const int grid = grid_rows(ex, n);
   if (ld == 4)
-    k_lobpcg_update<XT, 4><<<grid, 256, 0, ex.stream>>>(b, ctrl, n, init_mode);
+    k_lobpcg_update4<XT><<<grid_rows(ex, n * 4), 256, 0, ex.stream>>>(b, ctrl, n, init_mode);
   else if (ld == 8)
     k_lobpcg_update<XT, 8><<<grid, 256, 0, ex.stream>>>(b, ctrl, n, init_mode);
   else

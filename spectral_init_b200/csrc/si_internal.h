@@ -151,7 +151,7 @@ struct LobpcgCtrl {
 
 // One CTA: the small dense step of a LOBPCG iteration (or an init / plain
 // Rayleigh-Ritz / CholQR step).  gram: output of gram_dev SYM2 with ns blocks.
-void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode);
+void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode, int m);
 // Plain symmetric eigensolve / CholQR of an s x s matrix on the device (s <= SMAX):
 //   SM_RR_PLAIN: a (s x s) -> evals[s] ascending, evecs (s x s, columns)
 //   SM_CHOLQR:   a = B (s x s) -> evecs = L^-T (upper), evals[0] = 1 on success, 0 on failure

@@ -127,7 +127,7 @@ __device__ void cta_jacobi(double* A, double* V, int s, int ld, double* red, dou
     }
     off = cta_sum(off, red);
     dia = cta_sum(dia, red);
-    if (!(off > 1e-32 * (dia + off))) break;
+    if (!(off > DBL_EPSILON * DBL_EPSILON * dia)) break;
     for (int r = 0; r < s2 - 1; ++r) {
       for (int p = threadIdx.x; p < np; p += blockDim.x) {
         int a, b;
@@ -179,6 +179,16 @@ __device__ void cta_jacobi(double* A, double* V, int s, int ld, double* red, dou
         const double vx = V[k * ld + a], vy = V[k * ld + b];
         V[k * ld + a] = rc[p] * vx - rs[p] * vy;
         V[k * ld + b] = rs[p] * vx + rc[p] * vy;
+      }
+      __syncthreads();
+      // the rotation annihilates a_pq: store the exact zero (the two-phase
+      // update leaves O(eps) rounding there, which would never drop below the
+      // skip threshold and would keep every sweep rotating)
+      for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        if (rb[p] >= 0 && rs[p] != 0.0) {
+          A[ra[p] * ld + rb[p]] = 0.0;
+          A[rb[p] * ld + ra[p]] = 0.0;
+        }
       }
       __syncthreads();
     }
@@ -275,9 +285,9 @@ __device__ bool cta_rr_general(const double* gb, const double* ga, int P, const 
   return true;
 }
 
-__global__ void __launch_bounds__(ST) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
-                                                   int mode) {
-  extern __shared__ double smem[];
+// `ctrl` points to the CTA's shared-memory copy of the control block.
+__device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns, int mode,
+                                double* smem) {
   __shared__ double red[ST / 32];
   __shared__ double rc[SMAX / 2 + 1], rs[SMAX / 2 + 1], dsc[3 * MAXM], theta[MAXM], rn[MAXM];
   __shared__ int ra[SMAX / 2 + 1], rb[SMAX / 2 + 1], order[3 * MAXM], idx[3 * MAXM];
@@ -464,6 +474,24 @@ __global__ void __launch_bounds__(ST) k_small_step(LobpcgCtrl* ctrl, const doubl
   }
 }
 
+// The control block is staged in shared memory for the whole step (the step
+// is a long chain of small dependent updates) and written back at the end.
+__global__ void __launch_bounds__(ST) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
+                                                   int mode) {
+  extern __shared__ double smem[];
+  __shared__ LobpcgCtrl sctrl;
+  static_assert(sizeof(LobpcgCtrl) % sizeof(double) == 0, "control block must be a whole number of words");
+  constexpr int W = sizeof(LobpcgCtrl) / sizeof(double);
+  double* dst = reinterpret_cast<double*>(&sctrl);
+  const double* src = reinterpret_cast<const double*>(ctrl);
+  for (int i = threadIdx.x; i < W; i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  small_step_body(&sctrl, gram, ns, mode, smem);
+  __syncthreads();
+  double* back = reinterpret_cast<double*>(ctrl);
+  for (int i = threadIdx.x; i < W; i += blockDim.x) back[i] = dst[i];
+}
+
 __global__ void __launch_bounds__(ST) k_small_dense(const double* __restrict__ a, int s, int mode, double* evals,
                                                     double* evecs) {
   extern __shared__ double smem[];
@@ -503,7 +531,7 @@ __global__ void __launch_bounds__(ST) k_small_dense(const double* __restrict__ a
 
 }  // namespace
 
-void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode) {
+void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode, int m) {
   const int LDS = 3 * MAXM;
   const size_t smem = sizeof(double) * 4 * LDS * LDS;
   static bool attr_set[128] = {};
@@ -511,7 +539,9 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
     SI_CUDA(cudaFuncSetAttribute(k_small_step, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     attr_set[ex.device] = true;
   }
-  k_small_step<<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  // one warp is enough up to 8-wide blocks (problems of at most 24 x 24) and
+  // makes every barrier of the step a single-warp barrier
+  k_small_step<<<1, m <= 8 ? 32 : ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
   SI_LAUNCH_CHECK();
 }
 

@@ -113,25 +113,58 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
     const XT* blk[2] = {s.X.get(), s.AX.get()};
     gram_dev<XT>(ex, s.gw, GRAM_SYM2, blk, 1, 2, s.m, s.ld, s.n, s.gram.get());
   }
-  small_step_dev(ex, s.ctrl.get(), s.gram.get(), 1, SM_INIT);
+  small_step_dev(ex, s.ctrl.get(), s.gram.get(), 1, SM_INIT, s.m);
   lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 1);
   const XT* blk6[6] = {s.X.get(), s.R.get(), s.P.get(), s.AX.get(), s.AR.get(), s.AP.get()};
-  int batch = 4;
-  int launched = 0;
-  for (;;) {
-    for (int b = 0; b < batch; ++b) {
+  auto enqueue_iterations = [&](int count) {
+    for (int b = 0; b < count; ++b) {
       spmm_dev<XT>(ex, A, s.R.get(), s.AR.get(), s.ld, s.m, ep, s.stop(), f32vals);
       gram_dev<XT>(ex, s.gw, GRAM_SYM2, blk6, 3, 6, s.m, s.ld, s.n, s.gram.get(), s.stop());
-      small_step_dev(ex, s.ctrl.get(), s.gram.get(), 3, SM_ITER);
+      small_step_dev(ex, s.ctrl.get(), s.gram.get(), 3, SM_ITER, s.m);
       lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 0);
     }
-    launched += batch;
+  };
+  // One iteration's first pass allocates every work buffer; later batches are
+  // replayed from a captured CUDA graph (all kernel arguments are fixed for
+  // the solve, and the control state lives in device memory).
+  enqueue_iterations(1);
+  constexpr int kGraphBatch = 8;
+  cudaGraphExec_t exec = nullptr;
+  const uint64_t launches_before_capture = g_kernel_launches.load();
+  {
+    cudaGraph_t graph = nullptr;
+    SI_CUDA(cudaStreamBeginCapture(ex.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue_iterations(kGraphBatch);
+    } catch (...) {
+      cudaStreamEndCapture(ex.stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    SI_CUDA(cudaStreamEndCapture(ex.stream, &graph));
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    SI_CUDA(ie);
+  }
+  // captured launches are not executions; each graph replay adds its kernels below
+  const uint64_t per_replay = g_kernel_launches.load() - launches_before_capture;
+  g_kernel_launches.store(launches_before_capture);
+  struct ExecGuard {
+    cudaGraphExec_t e;
+    ~ExecGuard() {
+      if (e) cudaGraphExecDestroy(e);
+    }
+  } guard{exec};
+  int launched = 1;
+  for (;;) {
     int done = 0;
     SI_CUDA(cudaMemcpyAsync(&done, s.stop(), sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
     SI_CUDA(cudaStreamSynchronize(ex.stream));
     if (done) break;
-    SI_REQUIRE(launched <= maxiter + 8, SI_CUDA_ERROR, "lobpcg: device loop did not terminate");
-    batch = std::min(batch * 2, 32);
+    SI_REQUIRE(launched <= maxiter + 2 * kGraphBatch, SI_CUDA_ERROR, "lobpcg: device loop did not terminate");
+    SI_CUDA(cudaGraphLaunch(exec, ex.stream));
+    g_kernel_launches.fetch_add(per_replay);
+    launched += kGraphBatch;
   }
   SI_CUDA(cudaMemcpyAsync(&h, s.ctrl.get(), sizeof(h), cudaMemcpyDeviceToHost, ex.stream));
   SI_CUDA(cudaStreamSynchronize(ex.stream));
@@ -209,7 +242,7 @@ void rr_refine(const Exec& ex, const OpDev& L, LobpcgState<double>& s, const dou
   std::memset(&h, 0, sizeof(h));
   h.m = s.m;
   SI_CUDA(cudaMemcpyAsync(s.aux.get(), &h, sizeof(h), cudaMemcpyHostToDevice, ex.stream));
-  small_step_dev(ex, s.aux.get(), s.gram.get(), 1, SM_RR_PLAIN);
+  small_step_dev(ex, s.aux.get(), s.gram.get(), 1, SM_RR_PLAIN, s.m);
   const double* in[1] = {src};
   const double* coef[1] = {s.aux.get()->Cx};
   combine_dev<double>(ex, in, coef, 1, dst, s.m, s.m, MAXM, s.ld, s.n);

@@ -19,6 +19,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "si_internal.h"
 
@@ -87,6 +90,19 @@ struct RowLoad<float, 16> : RowLoadF32x8<16> {};
 template <int LD, int G>
 struct GroupReduce {
   static constexpr int W = (LD >= G) ? LD / G : 1;
+  // first output column owned by lane `sub` after run()
+  __device__ __forceinline__ static int base_of(int sub) {
+    int base = 0;
+    int width = LD;
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) {
+      if (width > W) {
+        if (sub & o) base += width / 2;
+        width /= 2;
+      }
+    }
+    return base;
+  }
   __device__ __forceinline__ static int run(double (&v)[LD], int sub, unsigned mask) {
     int base = 0;
     int width = LD;
@@ -129,46 +145,69 @@ __global__ void __launch_bounds__(256) k_spmm_vec(int64_t n, const uint64_t* __r
   constexpr int W = GroupReduce<LD, G>::W;
   const bool writer = (LD >= G) || ((sub & ((G / (LD < G ? LD : G)) - 1)) == 0);
 
-  for (int64_t row = group; row < n; row += ngroups) {
-    const uint64_t s = indptr[row];
-    const uint64_t e = indptr[row + 1];
+  // U entries per lane per pass: all index/value loads of a pass are issued
+  // before its gathers, and the next row's bounds are fetched while the
+  // current row is in flight, so each SM keeps many independent loads going
+  constexpr int U = (LD >= 16) ? 4 : 8;
+  int64_t row = group;
+  uint64_t s = 0, e = 0;
+  if (row < n) {
+    s = __ldg(indptr + row);
+    e = __ldg(indptr + row + 1);
+  }
+  for (; row < n; row += ngroups) {
+    const int64_t nrow = row + ngroups;
+    uint64_t ns = 0, ne = 0;
+    if (nrow < n) {
+      ns = __ldg(indptr + nrow);
+      ne = __ldg(indptr + nrow + 1);
+    }
+    // own-row epilogue terms, loaded up front so they overlap the gathers
+    const int obase = GroupReduce<LD, G>::base_of(sub);
+    double own[W], addz[W];
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      own[c] = 0.0;
+      addz[c] = 0.0;
+      if (writer) {
+        const int64_t off = row * LD + obase + c;
+        own[c] = diag * static_cast<double>(x[off]);
+        if (ep.z1) addz[c] = ep.beta * static_cast<double>(ep.z1[off]);
+        if (ep.z2) addz[c] = fma(ep.gamma, static_cast<double>(ep.z2[off]), addz[c]);
+        if (ep.z3) addz[c] = fma(ep.delta, static_cast<double>(ep.z3[off]), addz[c]);
+      }
+    }
     double acc[LD];
 #pragma unroll
     for (int c = 0; c < LD; ++c) acc[c] = 0.0;
-    uint64_t k = s + sub;
-    // two entries in flight per lane
-    for (; k + G < e; k += 2 * G) {
-      const uint32_t j0 = ld_stream(indices + k);
-      const uint32_t j1 = ld_stream(indices + k + G);
-      const double v0 = static_cast<double>(ld_stream(vals + k));
-      const double v1 = static_cast<double>(ld_stream(vals + k + G));
-      double x0[LD], x1[LD];
-      RowLoad<XT, LD>::run(x + static_cast<int64_t>(j0) * LD, x0);
-      RowLoad<XT, LD>::run(x + static_cast<int64_t>(j1) * LD, x1);
+    for (uint64_t b0 = s + sub; b0 < e; b0 += static_cast<uint64_t>(G) * U) {
+      uint32_t jj[U];
+      double vv[U];
 #pragma unroll
-      for (int c = 0; c < LD; ++c) acc[c] = fma(v0, x0[c], acc[c]);
+      for (int u = 0; u < U; ++u) {
+        const uint64_t k = b0 + static_cast<uint64_t>(u) * G;
+        const bool ok = k < e;
+        jj[u] = ok ? ld_stream(indices + k) : 0u;
+        vv[u] = ok ? static_cast<double>(ld_stream(vals + k)) : 0.0;
+      }
 #pragma unroll
-      for (int c = 0; c < LD; ++c) acc[c] = fma(v1, x1[c], acc[c]);
+      for (int u = 0; u < U; ++u) {
+        if (b0 + static_cast<uint64_t>(u) * G < e) {
+          double xr[LD];
+          RowLoad<XT, LD>::run(x + static_cast<int64_t>(jj[u]) * LD, xr);
+#pragma unroll
+          for (int c = 0; c < LD; ++c) acc[c] = fma(vv[u], xr[c], acc[c]);
+        }
+      }
     }
-    if (k < e) {
-      const uint32_t j0 = ld_stream(indices + k);
-      const double v0 = static_cast<double>(ld_stream(vals + k));
-      double x0[LD];
-      RowLoad<XT, LD>::run(x + static_cast<int64_t>(j0) * LD, x0);
-#pragma unroll
-      for (int c = 0; c < LD; ++c) acc[c] = fma(v0, x0[c], acc[c]);
-    }
+    s = ns;
+    e = ne;
     const int base = GroupReduce<LD, G>::run(acc, sub, mask);
     if (writer) {
 #pragma unroll
       for (int c = 0; c < W; ++c) {
         const int64_t off = row * LD + base + c;
-        double r = fma(diag, static_cast<double>(x[off]), acc[c]);
-        r *= ep.alpha;
-        if (ep.z1) r = fma(ep.beta, static_cast<double>(ep.z1[off]), r);
-        if (ep.z2) r = fma(ep.gamma, static_cast<double>(ep.z2[off]), r);
-        if (ep.z3) r = fma(ep.delta, static_cast<double>(ep.z3[off]), r);
-        y[off] = static_cast<XT>(r);
+        y[off] = static_cast<XT>(fma(ep.alpha, own[c] + acc[c], addz[c]));
       }
     }
   }
@@ -243,14 +282,76 @@ void launch_generic(const Exec& ex, const OpDev& op, const VT* vals, const XT* x
 }
 
 template <class VT, class XT, int LD>
-void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
-                const int* stop) {
-  switch (spmm_group_lanes(op)) {
+void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
+                  const int* stop) {
+  switch (g) {
     case 4: launch_vec<VT, XT, LD, 4>(ex, op, vals, x, y, ep, stop); break;
     case 8: launch_vec<VT, XT, LD, 8>(ex, op, vals, x, y, ep, stop); break;
     case 16: launch_vec<VT, XT, LD, 16>(ex, op, vals, x, y, ep, stop); break;
     default: launch_vec<VT, XT, LD, 32>(ex, op, vals, x, y, ep, stop); break;
   }
+}
+
+// Autotuner: lanes per row for one operator / block width / precision.  The
+// first call on a (device, operator, ld, value type, block type) times every
+// candidate with CUDA events on the caller's stream (the kernel is
+// idempotent: y never aliases its inputs) and caches the fastest; under
+// stream capture it uses the cached choice or the degree heuristic.
+struct TuneKey {
+  int device;
+  const void* indptr;
+  int64_t n, nnz;
+  int ld, vbytes, xbytes;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(device, indptr, n, nnz, ld, vbytes, xbytes) <
+           std::tie(o.device, o.indptr, o.n, o.nnz, o.ld, o.vbytes, o.xbytes);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+
+template <class VT, class XT, int LD>
+void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
+                const int* stop) {
+  const TuneKey key{ex.device, op.indptr, op.n, op.nnz, LD, static_cast<int>(sizeof(VT)),
+                    static_cast<int>(sizeof(XT))};
+  int g = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) g = it->second;
+  }
+  if (g == 0) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    SI_CUDA(cudaStreamIsCapturing(ex.stream, &cs));
+    const bool small = op.n < 20000;  // tiny operators: not worth timing
+    if (cs != cudaStreamCaptureStatusNone || small) {
+      g = spmm_group_lanes(op);
+    } else {
+      cudaEvent_t e0, e1;
+      SI_CUDA(cudaEventCreate(&e0));
+      SI_CUDA(cudaEventCreate(&e1));
+      float best = 1e30f;
+      for (int cand : {4, 8, 16, 32}) {
+        launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
+        SI_CUDA(cudaEventRecord(e0, ex.stream));
+        for (int r = 0; r < 3; ++r) launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
+        SI_CUDA(cudaEventRecord(e1, ex.stream));
+        SI_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        SI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+          best = ms;
+          g = cand;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = g;
+  }
+  launch_lanes<VT, XT, LD>(g, ex, op, vals, x, y, ep, stop);
 }
 
 template <class VT, class XT>
@@ -274,10 +375,12 @@ void dispatch(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* 
 }  // namespace
 
 int spmm_group_lanes(const OpDev& op) {
+  // a lane covers up to 8 entries per pass: fewest lanes that keep most rows
+  // to one pass (more rows in flight per SM beats wider groups)
   const double mean = op.n > 0 ? static_cast<double>(op.nnz) / static_cast<double>(op.n) : 0.0;
-  if (mean <= 6.0) return 4;
-  if (mean <= 20.0) return 8;
-  if (mean <= 56.0) return 16;
+  if (mean <= 28.0) return 4;
+  if (mean <= 56.0) return 8;
+  if (mean <= 112.0) return 16;
   return 32;
 }
 
