@@ -35,7 +35,23 @@ struct OpDev {
   const double* v64 = nullptr;
   const float* v32 = nullptr;
   double diag = 1.0;
+  // optional row partition for the tiled SpMM: block b covers rows
+  // [row_blocks[b], row_blocks[b+1]) (about kSpmmBlockNnz entries each)
+  const int64_t* row_blocks = nullptr;
+  int64_t n_blocks = 0;
 };
+
+constexpr int kSpmmBlockNnz = 1024;   // target entries per row block
+constexpr int kSpmmBlockCap = 2048;   // entries a block may hold in shared memory
+constexpr int kSpmmBlockRows = 1024;  // rows a block may hold in shared memory
+
+// Row partition of an operator for the tiled SpMM (device array of
+// n_blocks + 1 row starts, owned by the caller).
+struct RowBlocks {
+  DevBuf<int64_t> starts;
+  int64_t n_blocks = 0;
+};
+void make_row_blocks(const Exec& ex, const OpDev& op, RowBlocks& rb);
 
 // Epilogue of an SpMM: out = alpha * (A x) + beta * z1 + gamma * z2 + delta * z3
 // (z pointers share the layout of y; a null z contributes nothing).

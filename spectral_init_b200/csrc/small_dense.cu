@@ -118,6 +118,83 @@ __device__ void cta_jacobi(double* A, double* V, int s, int ld, double* red, dou
                            int* rb) {
   const int s2 = s + (s & 1);
   const int np = s2 / 2;
+  // this thread's (pair, index) items of a round, resolved once per call
+  constexpr int MAXIT = 12;
+  int itp[MAXIT], itk[MAXIT];
+  int nit = 0;
+  for (int t = threadIdx.x; t < np * s && nit < MAXIT; t += blockDim.x) {
+    itp[nit] = t / s;
+    itk[nit] = t % s;
+    ++nit;
+  }
+  const bool fast = np * s <= MAXIT * static_cast<int>(blockDim.x);
+  for (int sweep = 0; sweep < 40 && fast; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
+      const int i = t / s, j = t % s;
+      const double a = A[i * ld + j];
+      if (i == j) dia += a * a; else off += a * a;
+    }
+    off = cta_sum(off, red);
+    dia = cta_sum(dia, red);
+    if (!(off > DBL_EPSILON * DBL_EPSILON * dia)) return;
+    for (int r = 0; r < s2 - 1; ++r) {
+      for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        int a, b;
+        if (p == 0) {
+          a = r;
+          b = s2 - 1;
+        } else {
+          a = (r + p) % (s2 - 1);
+          b = (r - p + s2 - 1) % (s2 - 1);
+        }
+        if (a > b) {
+          const int t = a;
+          a = b;
+          b = t;
+        }
+        double c = 1.0, sn = 0.0;
+        if (b < s) {
+          const double apq = A[a * ld + b];
+          const double app = A[a * ld + a], aqq = A[b * ld + b];
+          if (fabs(apq) > 1e-300 && fabs(apq) > DBL_EPSILON * 1e-3 * sqrt(fabs(app * aqq))) {
+            const double theta = (aqq - app) / (2.0 * apq);
+            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            c = 1.0 / sqrt(t * t + 1.0);
+            sn = t * c;
+          }
+        }
+        rc[p] = c;
+        rs[p] = sn;
+        ra[p] = a;
+        rb[p] = (b < s && sn != 0.0) ? b : -1;
+      }
+      __syncthreads();
+      for (int q = 0; q < nit; ++q) {  // rows a, b
+        const int p = itp[q], k = itk[q];
+        const int a = ra[p], b = rb[p];
+        if (b < 0) continue;
+        const double x = A[a * ld + k], y = A[b * ld + k];
+        A[a * ld + k] = rc[p] * x - rs[p] * y;
+        A[b * ld + k] = rs[p] * x + rc[p] * y;
+      }
+      __syncthreads();
+      for (int q = 0; q < nit; ++q) {  // columns a, b (the annihilated pair set to exact zero)
+        const int p = itp[q], k = itk[q];
+        const int a = ra[p], b = rb[p];
+        if (b < 0) continue;
+        const double x = A[k * ld + a], y = A[k * ld + b];
+        A[k * ld + a] = (k == b) ? 0.0 : rc[p] * x - rs[p] * y;
+        A[k * ld + b] = (k == a) ? 0.0 : rs[p] * x + rc[p] * y;
+        const double vx = V[k * ld + a], vy = V[k * ld + b];
+        V[k * ld + a] = rc[p] * vx - rs[p] * vy;
+        V[k * ld + b] = rs[p] * vx + rc[p] * vy;
+      }
+      __syncthreads();
+    }
+  }
+  if (fast) return;
+  // wide problems (more items than the per-thread table holds): plain loops
   for (int sweep = 0; sweep < 40; ++sweep) {
     double off = 0.0, dia = 0.0;
     for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
@@ -539,9 +616,8 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
     SI_CUDA(cudaFuncSetAttribute(k_small_step, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     attr_set[ex.device] = true;
   }
-  // one warp is enough up to 8-wide blocks (problems of at most 24 x 24) and
-  // makes every barrier of the step a single-warp barrier
-  k_small_step<<<1, m <= 8 ? 32 : ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  (void)m;
+  k_small_step<<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
   SI_LAUNCH_CHECK();
 }
 

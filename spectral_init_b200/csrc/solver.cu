@@ -284,8 +284,16 @@ double max_eigenpair_residual_dev(const Exec& ex, const OpDev& op, const EigenRe
   return acc;
 }
 
-bool lobpcg_solve_dev(const Exec& ex, const OpDev& op, int n_components, uint64_t seed, bool regularize,
+bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64_t seed, bool regularize,
                       const double* sqrt_deg, const SolverConfig& cfg, EigenResult& out, SolverStats& st) {
+  // row partition for the tiled SpMM (built once per solve when absent)
+  RowBlocks row_blocks_;
+  OpDev op = op_in;
+  if (op.row_blocks == nullptr && op.n > 0) {
+    make_row_blocks(ex, op, row_blocks_);
+    op.row_blocks = row_blocks_.starts.get();
+    op.n_blocks = row_blocks_.n_blocks;
+  }
   const int64_t n = op.n;
   const int k = n_components + 1;
   if (n_components <= 0 || k >= n) return false;
@@ -440,8 +448,16 @@ int rsvd_k_sub(int64_t n, int rank) {
 
 }  // namespace
 
-void rsvd_solve_dev(const Exec& ex, const OpDev& op, int n_components, uint64_t seed, int oversampling, int nbiter,
+void rsvd_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64_t seed, int oversampling, int nbiter,
                     EigenResult& out, SolverStats& st) {
+  // row partition for the tiled SpMM (built once per solve when absent)
+  RowBlocks row_blocks_;
+  OpDev op = op_in;
+  if (op.row_blocks == nullptr && op.n > 0) {
+    make_row_blocks(ex, op, row_blocks_);
+    op.row_blocks = row_blocks_.starts.get();
+    op.n_blocks = row_blocks_.n_blocks;
+  }
   const int64_t n = op.n;
   SI_REQUIRE(n_components > 0 && n_components < n, SI_INVALID_ARGUMENT, "rsvd: need 0 < n_components < n");
   const int rank = n_components + 1;
@@ -506,8 +522,16 @@ void dense_evd_result(const Exec& ex, const OpDev& op, int k, EigenResult& out) 
   dense_evd_dev(ex, op, k, out.vals.data(), out.vecs.get(), k);
 }
 
-void solve_eigenproblem_dev(const Exec& ex, const OpDev& op, int n_components, uint64_t seed, const double* sqrt_deg,
+void solve_eigenproblem_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64_t seed, const double* sqrt_deg,
                             const SolverConfig& cfg, EigenResult& out, SolverStats& st) {
+  // row partition for the tiled SpMM (built once per solve when absent)
+  RowBlocks row_blocks_;
+  OpDev op = op_in;
+  if (op.row_blocks == nullptr && op.n > 0) {
+    make_row_blocks(ex, op, row_blocks_);
+    op.row_blocks = row_blocks_.starts.get();
+    op.n_blocks = row_blocks_.n_blocks;
+  }
   const int64_t n = op.n;
   const int k = n_components + 1;
   const int fl = cfg.force_level;

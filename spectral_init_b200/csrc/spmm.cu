@@ -22,6 +22,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <vector>
 
 #include "si_internal.h"
 
@@ -130,6 +131,91 @@ struct GroupReduce {
   }
 };
 
+// Where a row's index/value streams are read from.
+template <class VT>
+struct GlobalStream {
+  const uint32_t* idx;
+  const VT* val;
+  __device__ __forceinline__ uint32_t j(uint64_t k) const { return ld_stream(idx + k); }
+  __device__ __forceinline__ double v(uint64_t k) const { return static_cast<double>(ld_stream(val + k)); }
+};
+template <class VT>
+struct SharedStream {  // entries [base, base + count) staged in shared memory
+  const uint32_t* idx;
+  const VT* val;
+  uint64_t base;
+  __device__ __forceinline__ uint32_t j(uint64_t k) const { return idx[k - base]; }
+  __device__ __forceinline__ double v(uint64_t k) const { return static_cast<double>(val[k - base]); }
+};
+
+// One row of y = epilogue(A x) by a group of G lanes.  U entries per lane per
+// pass: all index/value reads of a pass are issued before its gathers.  The
+// own-row epilogue terms are loaded first so they overlap the gathers.
+template <class VT, class XT, int LD, int G, class Src>
+__device__ __forceinline__ void spmm_row(int64_t row, uint64_t s, uint64_t e, const Src& src, double diag,
+                                         const XT* __restrict__ x, XT* __restrict__ y, const Epilogue<XT>& ep,
+                                         int sub, unsigned mask, bool writer) {
+  constexpr int W = GroupReduce<LD, G>::W;
+  constexpr int U = (LD >= 16) ? 4 : 8;
+  const int obase = GroupReduce<LD, G>::base_of(sub);
+  double own[W], addz[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) {
+    own[c] = 0.0;
+    addz[c] = 0.0;
+    if (writer) {
+      const int64_t off = row * LD + obase + c;
+      own[c] = diag * static_cast<double>(x[off]);
+      if (ep.z1) addz[c] = ep.beta * static_cast<double>(ep.z1[off]);
+      if (ep.z2) addz[c] = fma(ep.gamma, static_cast<double>(ep.z2[off]), addz[c]);
+      if (ep.z3) addz[c] = fma(ep.delta, static_cast<double>(ep.z3[off]), addz[c]);
+    }
+  }
+  double acc[LD];
+#pragma unroll
+  for (int c = 0; c < LD; ++c) acc[c] = 0.0;
+  for (uint64_t b0 = s + sub; b0 < e; b0 += static_cast<uint64_t>(G) * U) {
+    uint32_t jj[U];
+    double vv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t k = b0 + static_cast<uint64_t>(u) * G;
+      const bool ok = k < e;
+      jj[u] = ok ? src.j(k) : 0u;
+      vv[u] = ok ? src.v(k) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (b0 + static_cast<uint64_t>(u) * G < e) {
+        double xr[LD];
+        RowLoad<XT, LD>::run(x + static_cast<int64_t>(jj[u]) * LD, xr);
+#pragma unroll
+        for (int c = 0; c < LD; ++c) acc[c] = fma(vv[u], xr[c], acc[c]);
+      }
+    }
+  }
+  const int base = GroupReduce<LD, G>::run(acc, sub, mask);
+  if (writer) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      const int64_t off = row * LD + base + c;
+      y[off] = static_cast<XT>(fma(ep.alpha, own[c] + acc[c], addz[c]));
+    }
+  }
+}
+
+template <int G>
+__device__ __forceinline__ unsigned group_mask(int lane) {
+  return (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+}
+
+template <int LD, int G>
+__device__ __forceinline__ bool group_writer(int sub) {
+  return (LD >= G) || ((sub & ((G / (LD < G ? LD : G)) - 1)) == 0);
+}
+
+// Direct kernel: rows in grid-stride order, streams read from global memory;
+// the next row's bounds are fetched while the current row is in flight.
 template <class VT, class XT, int LD, int G>
 __global__ void __launch_bounds__(256) k_spmm_vec(int64_t n, const uint64_t* __restrict__ indptr,
                                                   const uint32_t* __restrict__ indices,
@@ -139,16 +225,11 @@ __global__ void __launch_bounds__(256) k_spmm_vec(int64_t n, const uint64_t* __r
   if (stop != nullptr && *stop != 0) return;
   const int lane = threadIdx.x & 31;
   const int sub = lane & (G - 1);
-  const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+  const unsigned mask = group_mask<G>(lane);
+  const bool writer = group_writer<LD, G>(sub);
   const int64_t group = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G;
   const int64_t ngroups = static_cast<int64_t>(gridDim.x) * blockDim.x / G;
-  constexpr int W = GroupReduce<LD, G>::W;
-  const bool writer = (LD >= G) || ((sub & ((G / (LD < G ? LD : G)) - 1)) == 0);
-
-  // U entries per lane per pass: all index/value loads of a pass are issued
-  // before its gathers, and the next row's bounds are fetched while the
-  // current row is in flight, so each SM keeps many independent loads going
-  constexpr int U = (LD >= 16) ? 4 : 8;
+  const GlobalStream<VT> src{indices, vals};
   int64_t row = group;
   uint64_t s = 0, e = 0;
   if (row < n) {
@@ -162,54 +243,136 @@ __global__ void __launch_bounds__(256) k_spmm_vec(int64_t n, const uint64_t* __r
       ns = __ldg(indptr + nrow);
       ne = __ldg(indptr + nrow + 1);
     }
-    // own-row epilogue terms, loaded up front so they overlap the gathers
-    const int obase = GroupReduce<LD, G>::base_of(sub);
-    double own[W], addz[W];
-#pragma unroll
-    for (int c = 0; c < W; ++c) {
-      own[c] = 0.0;
-      addz[c] = 0.0;
-      if (writer) {
-        const int64_t off = row * LD + obase + c;
-        own[c] = diag * static_cast<double>(x[off]);
-        if (ep.z1) addz[c] = ep.beta * static_cast<double>(ep.z1[off]);
-        if (ep.z2) addz[c] = fma(ep.gamma, static_cast<double>(ep.z2[off]), addz[c]);
-        if (ep.z3) addz[c] = fma(ep.delta, static_cast<double>(ep.z3[off]), addz[c]);
-      }
-    }
-    double acc[LD];
-#pragma unroll
-    for (int c = 0; c < LD; ++c) acc[c] = 0.0;
-    for (uint64_t b0 = s + sub; b0 < e; b0 += static_cast<uint64_t>(G) * U) {
-      uint32_t jj[U];
-      double vv[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const uint64_t k = b0 + static_cast<uint64_t>(u) * G;
-        const bool ok = k < e;
-        jj[u] = ok ? ld_stream(indices + k) : 0u;
-        vv[u] = ok ? static_cast<double>(ld_stream(vals + k)) : 0.0;
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (b0 + static_cast<uint64_t>(u) * G < e) {
-          double xr[LD];
-          RowLoad<XT, LD>::run(x + static_cast<int64_t>(jj[u]) * LD, xr);
-#pragma unroll
-          for (int c = 0; c < LD; ++c) acc[c] = fma(vv[u], xr[c], acc[c]);
-        }
-      }
-    }
+    spmm_row<VT, XT, LD, G>(row, s, e, src, diag, x, y, ep, sub, mask, writer);
     s = ns;
     e = ne;
-    const int base = GroupReduce<LD, G>::run(acc, sub, mask);
-    if (writer) {
-#pragma unroll
-      for (int c = 0; c < W; ++c) {
-        const int64_t off = row * LD + base + c;
-        y[off] = static_cast<XT>(fma(ep.alpha, own[c] + acc[c], addz[c]));
-      }
+  }
+}
+
+// Tiled kernel: persistent CTAs walk row blocks of ~kSpmmBlockNnz entries.
+// A block's row pointers, column indices and values are staged into shared
+// memory with cp.async (every warp request a full contiguous 128-byte line)
+// while the previous block is computed from shared memory, so the only global
+// loads of the compute phase are the x-row gathers (L2 resident).  Blocks
+// that do not fit (a row longer than the staging capacity) are computed
+// straight from global memory.
+__device__ __forceinline__ void cp_async_4(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_8(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit_grp() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_grp() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+template <class VT>
+struct TileSmem {
+  uint32_t idx[2][kSpmmBlockCap];
+  VT val[2][kSpmmBlockCap];
+  uint64_t ptr[2][kSpmmBlockRows + 1];
+};
+
+template <class VT, class XT, int LD, int G>
+__global__ void __launch_bounds__(256) k_spmm_tiled(int64_t n, const uint64_t* __restrict__ indptr,
+                                                    const uint32_t* __restrict__ indices,
+                                                    const VT* __restrict__ vals, const int64_t* __restrict__ rblk,
+                                                    int64_t nblk, double diag, const XT* __restrict__ x,
+                                                    XT* __restrict__ y, Epilogue<XT> ep,
+                                                    const int* __restrict__ stop) {
+  if (stop != nullptr && *stop != 0) return;
+  extern __shared__ __align__(16) unsigned char tile_raw[];
+  TileSmem<VT>& sm = *reinterpret_cast<TileSmem<VT>*>(tile_raw);
+  const int lane = threadIdx.x & 31;
+  const int sub = lane & (G - 1);
+  const unsigned mask = group_mask<G>(lane);
+  const bool writer = group_writer<LD, G>(sub);
+  const int group = threadIdx.x / G;
+  constexpr int NG = 256 / G;
+
+  // bounds of a block and whether it is staged
+  auto block_info = [&](int64_t b, int64_t& r0, int64_t& r1, uint64_t& p0, uint64_t& p1) {
+    r0 = rblk[b];
+    r1 = rblk[b + 1];
+    p0 = indptr[r0];
+    p1 = indptr[r1];
+    return (r1 - r0) <= kSpmmBlockRows && (p1 - p0) <= static_cast<uint64_t>(kSpmmBlockCap);
+  };
+  auto stage = [&](int64_t r0, int64_t r1, uint64_t p0, uint64_t p1, int buf) {
+    const int ne = static_cast<int>(p1 - p0);
+    const int nr = static_cast<int>(r1 - r0);
+    for (int t = threadIdx.x; t < ne; t += 256) {
+      cp_async_4(&sm.idx[buf][t], indices + p0 + t);
+      if constexpr (sizeof(VT) == 8) cp_async_8(&sm.val[buf][t], vals + p0 + t);
+      else cp_async_4(&sm.val[buf][t], vals + p0 + t);
     }
+    for (int t = threadIdx.x; t <= nr; t += 256) cp_async_8(&sm.ptr[buf][t], indptr + r0 + t);
+  };
+
+  int64_t b = blockIdx.x;
+  int buf = 0;
+  int64_t r0 = 0, r1 = 0;
+  uint64_t p0 = 0, p1 = 0;
+  bool fits = false;
+  if (b < nblk) {
+    fits = block_info(b, r0, r1, p0, p1);
+    if (fits) stage(r0, r1, p0, p1, 0);
+  }
+  cp_async_commit_grp();
+  for (; b < nblk; b += gridDim.x) {
+    const int64_t bn = b + gridDim.x;
+    int64_t nr0 = 0, nr1 = 0;
+    uint64_t np0 = 0, np1 = 0;
+    bool nfits = false;
+    if (bn < nblk) {
+      nfits = block_info(bn, nr0, nr1, np0, np1);
+      if (nfits) stage(nr0, nr1, np0, np1, buf ^ 1);
+    }
+    cp_async_commit_grp();
+    cp_async_wait_grp<1>();
+    __syncthreads();
+    const int nr = static_cast<int>(r1 - r0);
+    if (fits) {
+      const SharedStream<VT> src{sm.idx[buf], sm.val[buf], p0};
+      for (int rr = group; rr < nr; rr += NG)
+        spmm_row<VT, XT, LD, G>(r0 + rr, sm.ptr[buf][rr], sm.ptr[buf][rr + 1], src, diag, x, y, ep, sub, mask,
+                                writer);
+    } else {
+      const GlobalStream<VT> src{indices, vals};
+      for (int64_t rr = group; rr < r1 - r0; rr += NG)
+        spmm_row<VT, XT, LD, G>(r0 + rr, indptr[r0 + rr], indptr[r0 + rr + 1], src, diag, x, y, ep, sub, mask,
+                                writer);
+    }
+    __syncthreads();
+    buf ^= 1;
+    r0 = nr0;
+    r1 = nr1;
+    p0 = np0;
+    p1 = np1;
+    fits = nfits;
+  }
+  cp_async_wait_grp<0>();
+}
+
+// row_blocks[b] = first row whose start offset is >= b * kSpmmBlockNnz
+__global__ void k_row_blocks(int64_t n, const uint64_t* __restrict__ indptr, int64_t nblk, int64_t* out) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b <= nblk; b += stride) {
+    if (b == nblk) {
+      out[b] = n;
+      continue;
+    }
+    const uint64_t target = static_cast<uint64_t>(b) * kSpmmBlockNnz;
+    int64_t lo = 0, hi = n;  // first r in [0, n] with indptr[r] >= target
+    while (lo < hi) {
+      const int64_t mid = lo + (hi - lo) / 2;
+      if (indptr[mid] >= target) hi = mid; else lo = mid + 1;
+    }
+    out[b] = lo;
   }
 }
 
@@ -281,6 +444,26 @@ void launch_generic(const Exec& ex, const OpDev& op, const VT* vals, const XT* x
   SI_LAUNCH_CHECK();
 }
 
+template <class VT, class XT, int LD, int G>
+void launch_tiled(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
+                  const int* stop) {
+  const int smem = static_cast<int>(sizeof(TileSmem<VT>));
+  static int resident[128] = {};  // per device: resident CTAs per SM (0 = not set up)
+  const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
+  if (resident[dev] == 0) {
+    SI_CUDA(cudaFuncSetAttribute(k_spmm_tiled<VT, XT, LD, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmm_tiled<VT, XT, LD, G>, 256, smem));
+    resident[dev] = std::max(per_sm, 1);
+  }
+  const int grid = static_cast<int>(
+      std::max<int64_t>(1, std::min<int64_t>(op.n_blocks, int64_t(ex.sms) * resident[dev])));
+  k_spmm_tiled<VT, XT, LD, G><<<grid, 256, smem, ex.stream>>>(op.n, op.indptr, op.indices, vals, op.row_blocks,
+                                                               op.n_blocks, op.diag, x, y, ep, stop);
+  SI_LAUNCH_CHECK();
+}
+
+// choice < 100: direct kernel with `choice` lanes per row; 100 + g: tiled kernel
 template <class VT, class XT, int LD>
 void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                   const int* stop) {
@@ -288,6 +471,8 @@ void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const 
     case 4: launch_vec<VT, XT, LD, 4>(ex, op, vals, x, y, ep, stop); break;
     case 8: launch_vec<VT, XT, LD, 8>(ex, op, vals, x, y, ep, stop); break;
     case 16: launch_vec<VT, XT, LD, 16>(ex, op, vals, x, y, ep, stop); break;
+    case 104: launch_tiled<VT, XT, LD, 4>(ex, op, vals, x, y, ep, stop); break;
+    case 108: launch_tiled<VT, XT, LD, 8>(ex, op, vals, x, y, ep, stop); break;
     default: launch_vec<VT, XT, LD, 32>(ex, op, vals, x, y, ep, stop); break;
   }
 }
@@ -301,10 +486,10 @@ struct TuneKey {
   int device;
   const void* indptr;
   int64_t n, nnz;
-  int ld, vbytes, xbytes;
+  int ld, vbytes, xbytes, tiled;
   bool operator<(const TuneKey& o) const {
-    return std::tie(device, indptr, n, nnz, ld, vbytes, xbytes) <
-           std::tie(o.device, o.indptr, o.n, o.nnz, o.ld, o.vbytes, o.xbytes);
+    return std::tie(device, indptr, n, nnz, ld, vbytes, xbytes, tiled) <
+           std::tie(o.device, o.indptr, o.n, o.nnz, o.ld, o.vbytes, o.xbytes, o.tiled);
   }
 };
 std::mutex g_tune_mu;
@@ -313,8 +498,9 @@ std::map<TuneKey, int> g_tune;
 template <class VT, class XT, int LD>
 void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                 const int* stop) {
+  const bool tiled = op.row_blocks != nullptr && op.n_blocks > 0;
   const TuneKey key{ex.device, op.indptr, op.n, op.nnz, LD, static_cast<int>(sizeof(VT)),
-                    static_cast<int>(sizeof(XT))};
+                    static_cast<int>(sizeof(XT)), tiled ? 1 : 0};
   int g = 0;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -326,13 +512,18 @@ void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT
     SI_CUDA(cudaStreamIsCapturing(ex.stream, &cs));
     const bool small = op.n < 20000;  // tiny operators: not worth timing
     if (cs != cudaStreamCaptureStatusNone || small) {
-      g = spmm_group_lanes(op);
+      g = tiled ? 104 : spmm_group_lanes(op);
     } else {
       cudaEvent_t e0, e1;
       SI_CUDA(cudaEventCreate(&e0));
       SI_CUDA(cudaEventCreate(&e1));
       float best = 1e30f;
-      for (int cand : {4, 8, 16, 32}) {
+      std::vector<int> cands = {4, 8, 16, 32};
+      if (tiled) {
+        cands.push_back(104);
+        cands.push_back(108);
+      }
+      for (int cand : cands) {
         launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
         SI_CUDA(cudaEventRecord(e0, ex.stream));
         for (int r = 0; r < 3; ++r) launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
@@ -373,6 +564,14 @@ void dispatch(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* 
 }
 
 }  // namespace
+
+void make_row_blocks(const Exec& ex, const OpDev& op, RowBlocks& rb) {
+  rb.n_blocks = std::max<int64_t>(1, (op.nnz + kSpmmBlockNnz - 1) / kSpmmBlockNnz);
+  rb.starts.alloc(rb.n_blocks + 1, ex.stream);
+  const int grid = static_cast<int>(std::min<int64_t>((rb.n_blocks + 256) / 256, int64_t(ex.sms) * 8));
+  k_row_blocks<<<std::max(grid, 1), 256, 0, ex.stream>>>(op.n, op.indptr, rb.n_blocks, rb.starts.get());
+  SI_LAUNCH_CHECK();
+}
 
 int spmm_group_lanes(const OpDev& op) {
   // a lane covers up to 8 entries per pass: fewest lanes that keep most rows
