@@ -359,8 +359,7 @@ si_status si_spmm(si_ctx* ctx, const si_operator* op, const double* x, double* y
     SI_REQUIRE(k >= 1, SI_INVALID_ARGUMENT, "k must be >= 1");
     si::RowBlocks rb;
     si::make_row_blocks(ex, o, rb);
-    o.row_blocks = rb.starts.get();
-    o.n_blocks = rb.n_blocks;
+    rb.attach(o);
     si::Epilogue<double> ep;
     si::spmm_dev<double>(ex, o, x, y, static_cast<int>(k), static_cast<int>(k), ep);
     SI_CUDA(cudaStreamSynchronize(ex.stream));
@@ -374,8 +373,7 @@ si_status si_spmm_f32(si_ctx* ctx, const si_operator* op, const float* x, float*
     SI_REQUIRE(k >= 1, SI_INVALID_ARGUMENT, "k must be >= 1");
     si::RowBlocks rb;
     si::make_row_blocks(ex, o, rb);
-    o.row_blocks = rb.starts.get();
-    o.n_blocks = rb.n_blocks;
+    rb.attach(o);
     si::Epilogue<float> ep;
     si::spmm_dev<float>(ex, o, x, y, static_cast<int>(k), static_cast<int>(k), ep, nullptr, true);
     SI_CUDA(cudaStreamSynchronize(ex.stream));

@@ -38,6 +38,7 @@ struct OpDev {
   // optional row partition for the tiled SpMM: block b covers rows
   // [row_blocks[b], row_blocks[b+1]) (about kSpmmBlockNnz entries each)
   const int64_t* row_blocks = nullptr;
+  const uint64_t* block_ptr = nullptr;  // indptr[row_blocks[b]]
   int64_t n_blocks = 0;
 };
 
@@ -49,7 +50,13 @@ constexpr int kSpmmBlockRows = 1024;  // rows a block may hold in shared memory
 // n_blocks + 1 row starts, owned by the caller).
 struct RowBlocks {
   DevBuf<int64_t> starts;
+  DevBuf<uint64_t> ptrs;
   int64_t n_blocks = 0;
+  void attach(OpDev& op) const {
+    op.row_blocks = starts.get();
+    op.block_ptr = ptrs.get();
+    op.n_blocks = n_blocks;
+  }
 };
 void make_row_blocks(const Exec& ex, const OpDev& op, RowBlocks& rb);
 

@@ -291,8 +291,7 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
   OpDev op = op_in;
   if (op.row_blocks == nullptr && op.n > 0) {
     make_row_blocks(ex, op, row_blocks_);
-    op.row_blocks = row_blocks_.starts.get();
-    op.n_blocks = row_blocks_.n_blocks;
+    row_blocks_.attach(op);
   }
   const int64_t n = op.n;
   const int k = n_components + 1;
@@ -455,8 +454,7 @@ void rsvd_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64
   OpDev op = op_in;
   if (op.row_blocks == nullptr && op.n > 0) {
     make_row_blocks(ex, op, row_blocks_);
-    op.row_blocks = row_blocks_.starts.get();
-    op.n_blocks = row_blocks_.n_blocks;
+    row_blocks_.attach(op);
   }
   const int64_t n = op.n;
   SI_REQUIRE(n_components > 0 && n_components < n, SI_INVALID_ARGUMENT, "rsvd: need 0 < n_components < n");
@@ -529,8 +527,7 @@ void solve_eigenproblem_dev(const Exec& ex, const OpDev& op_in, int n_components
   OpDev op = op_in;
   if (op.row_blocks == nullptr && op.n > 0) {
     make_row_blocks(ex, op, row_blocks_);
-    op.row_blocks = row_blocks_.starts.get();
-    op.n_blocks = row_blocks_.n_blocks;
+    row_blocks_.attach(op);
   }
   const int64_t n = op.n;
   const int k = n_components + 1;

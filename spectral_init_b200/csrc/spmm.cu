@@ -277,12 +277,20 @@ struct TileSmem {
   uint64_t ptr[2][kSpmmBlockRows + 1];
 };
 
+struct BlockInfo {
+  int64_t r0 = 0, r1 = 0;
+  uint64_t p0 = 0, p1 = 0;
+  __device__ bool fits() const {
+    return (r1 - r0) <= kSpmmBlockRows && (p1 - p0) <= static_cast<uint64_t>(kSpmmBlockCap);
+  }
+};
+
 template <class VT, class XT, int LD, int G>
 __global__ void __launch_bounds__(256) k_spmm_tiled(int64_t n, const uint64_t* __restrict__ indptr,
                                                     const uint32_t* __restrict__ indices,
                                                     const VT* __restrict__ vals, const int64_t* __restrict__ rblk,
-                                                    int64_t nblk, double diag, const XT* __restrict__ x,
-                                                    XT* __restrict__ y, Epilogue<XT> ep,
+                                                    const uint64_t* __restrict__ bptr, int64_t nblk, double diag,
+                                                    const XT* __restrict__ x, XT* __restrict__ y, Epilogue<XT> ep,
                                                     const int* __restrict__ stop) {
   if (stop != nullptr && *stop != 0) return;
   extern __shared__ __align__(16) unsigned char tile_raw[];
@@ -294,68 +302,66 @@ __global__ void __launch_bounds__(256) k_spmm_tiled(int64_t n, const uint64_t* _
   const int group = threadIdx.x / G;
   constexpr int NG = 256 / G;
 
-  // bounds of a block and whether it is staged
-  auto block_info = [&](int64_t b, int64_t& r0, int64_t& r1, uint64_t& p0, uint64_t& p1) {
-    r0 = rblk[b];
-    r1 = rblk[b + 1];
-    p0 = indptr[r0];
-    p1 = indptr[r1];
-    return (r1 - r0) <= kSpmmBlockRows && (p1 - p0) <= static_cast<uint64_t>(kSpmmBlockCap);
-  };
-  auto stage = [&](int64_t r0, int64_t r1, uint64_t p0, uint64_t p1, int buf) {
-    const int ne = static_cast<int>(p1 - p0);
-    const int nr = static_cast<int>(r1 - r0);
-    for (int t = threadIdx.x; t < ne; t += 256) {
-      cp_async_4(&sm.idx[buf][t], indices + p0 + t);
-      if constexpr (sizeof(VT) == 8) cp_async_8(&sm.val[buf][t], vals + p0 + t);
-      else cp_async_4(&sm.val[buf][t], vals + p0 + t);
+  // block bounds: four independent loads (row range and its entry range)
+  auto info = [&](int64_t b) {
+    BlockInfo bi;
+    if (b < nblk) {
+      bi.r0 = rblk[b];
+      bi.r1 = rblk[b + 1];
+      bi.p0 = bptr[b];
+      bi.p1 = bptr[b + 1];
     }
-    for (int t = threadIdx.x; t <= nr; t += 256) cp_async_8(&sm.ptr[buf][t], indptr + r0 + t);
+    return bi;
+  };
+  auto stage = [&](const BlockInfo& bi, int buf) {
+    const int ne = static_cast<int>(bi.p1 - bi.p0);
+    const int nr = static_cast<int>(bi.r1 - bi.r0);
+    for (int t = threadIdx.x; t < ne; t += 256) {
+      cp_async_4(&sm.idx[buf][t], indices + bi.p0 + t);
+      if constexpr (sizeof(VT) == 8) cp_async_8(&sm.val[buf][t], vals + bi.p0 + t);
+      else cp_async_4(&sm.val[buf][t], vals + bi.p0 + t);
+    }
+    for (int t = threadIdx.x; t <= nr; t += 256) cp_async_8(&sm.ptr[buf][t], indptr + bi.r0 + t);
   };
 
   int64_t b = blockIdx.x;
+  const int64_t step = gridDim.x;
   int buf = 0;
-  int64_t r0 = 0, r1 = 0;
-  uint64_t p0 = 0, p1 = 0;
-  bool fits = false;
-  if (b < nblk) {
-    fits = block_info(b, r0, r1, p0, p1);
-    if (fits) stage(r0, r1, p0, p1, 0);
-  }
+  BlockInfo cur = info(b);
+  if (b < nblk && cur.fits()) stage(cur, 0);
   cp_async_commit_grp();
-  for (; b < nblk; b += gridDim.x) {
-    const int64_t bn = b + gridDim.x;
-    int64_t nr0 = 0, nr1 = 0;
-    uint64_t np0 = 0, np1 = 0;
-    bool nfits = false;
-    if (bn < nblk) {
-      nfits = block_info(bn, nr0, nr1, np0, np1);
-      if (nfits) stage(nr0, nr1, np0, np1, buf ^ 1);
-    }
+  BlockInfo nxt = info(b + step);
+  for (; b < nblk; b += step) {
+    if (b + step < nblk && nxt.fits()) stage(nxt, buf ^ 1);
     cp_async_commit_grp();
+    const BlockInfo after = info(b + 2 * step);  // in flight during this block's compute
     cp_async_wait_grp<1>();
     __syncthreads();
-    const int nr = static_cast<int>(r1 - r0);
-    if (fits) {
-      const SharedStream<VT> src{sm.idx[buf], sm.val[buf], p0};
+    if (cur.fits()) {
+      const int nr = static_cast<int>(cur.r1 - cur.r0);
+      const SharedStream<VT> src{sm.idx[buf], sm.val[buf], cur.p0};
       for (int rr = group; rr < nr; rr += NG)
-        spmm_row<VT, XT, LD, G>(r0 + rr, sm.ptr[buf][rr], sm.ptr[buf][rr + 1], src, diag, x, y, ep, sub, mask,
+        spmm_row<VT, XT, LD, G>(cur.r0 + rr, sm.ptr[buf][rr], sm.ptr[buf][rr + 1], src, diag, x, y, ep, sub, mask,
                                 writer);
     } else {
       const GlobalStream<VT> src{indices, vals};
-      for (int64_t rr = group; rr < r1 - r0; rr += NG)
-        spmm_row<VT, XT, LD, G>(r0 + rr, indptr[r0 + rr], indptr[r0 + rr + 1], src, diag, x, y, ep, sub, mask,
-                                writer);
+      for (int64_t rr = group; rr < cur.r1 - cur.r0; rr += NG)
+        spmm_row<VT, XT, LD, G>(cur.r0 + rr, indptr[cur.r0 + rr], indptr[cur.r0 + rr + 1], src, diag, x, y, ep, sub,
+                                mask, writer);
     }
     __syncthreads();
     buf ^= 1;
-    r0 = nr0;
-    r1 = nr1;
-    p0 = np0;
-    p1 = np1;
-    fits = nfits;
+    cur = nxt;
+    nxt = after;
   }
   cp_async_wait_grp<0>();
+}
+
+__global__ void k_block_ptrs(int64_t nblk, const int64_t* __restrict__ rblk, const uint64_t* __restrict__ indptr,
+                             uint64_t* __restrict__ out) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b <= nblk; b += stride)
+    out[b] = indptr[rblk[b]];
 }
 
 // row_blocks[b] = first row whose start offset is >= b * kSpmmBlockNnz
@@ -459,7 +465,7 @@ void launch_tiled(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, 
   const int grid = static_cast<int>(
       std::max<int64_t>(1, std::min<int64_t>(op.n_blocks, int64_t(ex.sms) * resident[dev])));
   k_spmm_tiled<VT, XT, LD, G><<<grid, 256, smem, ex.stream>>>(op.n, op.indptr, op.indices, vals, op.row_blocks,
-                                                               op.n_blocks, op.diag, x, y, ep, stop);
+                                                               op.block_ptr, op.n_blocks, op.diag, x, y, ep, stop);
   SI_LAUNCH_CHECK();
 }
 
@@ -570,6 +576,9 @@ void make_row_blocks(const Exec& ex, const OpDev& op, RowBlocks& rb) {
   rb.starts.alloc(rb.n_blocks + 1, ex.stream);
   const int grid = static_cast<int>(std::min<int64_t>((rb.n_blocks + 256) / 256, int64_t(ex.sms) * 8));
   k_row_blocks<<<std::max(grid, 1), 256, 0, ex.stream>>>(op.n, op.indptr, rb.n_blocks, rb.starts.get());
+  SI_LAUNCH_CHECK();
+  rb.ptrs.alloc(rb.n_blocks + 1, ex.stream);
+  k_block_ptrs<<<std::max(grid, 1), 256, 0, ex.stream>>>(rb.n_blocks, rb.starts.get(), op.indptr, rb.ptrs.get());
   SI_LAUNCH_CHECK();
 }
 
