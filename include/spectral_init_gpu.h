@@ -220,6 +220,21 @@ si_status si_dense_evd_host(si_ctx* ctx, const si_csr_f64* laplacian, uint32_t k
 /* normalize_signs (src/scaling.rs:62-74) on a DEVICE f64 block [n x k]. */
 si_status si_normalize_signs(si_ctx* ctx, double* coords, uint64_t n, uint32_t k);
 
+/* No counterpart in the reference.  The same sign normalisation as
+ * si_normalize_signs on a DEVICE f64 block [n x k], for callers that cannot
+ * let a library allocate device memory: a process whose HBM is already
+ * reserved by another allocator (a serving engine or framework caching
+ * allocator), or a latency-bound loop where an allocation or free on a shared
+ * device may stall other streams.  It calls no cudaMalloc, cudaFree or pool
+ * allocation: its temporaries live in one static device array of about
+ * 513 KiB that every device loading the library holds until exit, which
+ * limits k to 64 columns (larger k returns SI_INVALID_ARGUMENT); n is
+ * unbounded.  The first call on a device looks up that array's device
+ * address, so make it before any stream capture.  All calls on a device share
+ * the array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  Returns after the stream has finished the work. */
+si_status si_normalize_signs_noalloc(si_ctx* ctx, double* coords, uint64_t n, uint32_t k);
+
 /* scale_and_add_noise (src/scaling.rs:78-89): DEVICE f64 [n x k] -> DEVICE f32
  * [n x k]: max-|.| scaled to 10, plus N(0, 1e-4) noise from `seed`. */
 si_status si_scale_and_add_noise(si_ctx* ctx, const double* coords, uint64_t n, uint32_t k,

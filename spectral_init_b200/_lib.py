@@ -89,6 +89,7 @@ _SIGNATURES = {
                                      vp, vp]),
     "si_dense_evd_host": (C.c_int, [vp, C.POINTER(SiCsrF64), C.c_uint32, vp, vp]),
     "si_normalize_signs": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32]),
+    "si_normalize_signs_noalloc": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32]),
     "si_scale_and_add_noise": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32, C.c_uint64, vp]),
 }
 

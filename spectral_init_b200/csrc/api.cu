@@ -495,6 +495,22 @@ si_status si_normalize_signs(si_ctx* ctx, double* coords, uint64_t n, uint32_t k
   });
 }
 
+// Same result as si_normalize_signs, with every temporary in a static device
+// array instead of pool allocations (noalloc.cu explains who needs this).
+si_status si_normalize_signs_noalloc(si_ctx* ctx, double* coords, uint64_t n, uint32_t k) {
+  return guarded(ctx, [&] {
+    const si::Exec ex = ctx->ex();
+    if (n > static_cast<uint64_t>(INT64_MAX))
+      throw si::Error(SI_INVALID_ARGUMENT, "normalize_signs_noalloc: n does not fit a 64-bit signed index");
+    if (k > static_cast<uint32_t>(si::kNoAllocMaxCols))
+      throw si::Error(SI_INVALID_ARGUMENT, "normalize_signs_noalloc: k = " + std::to_string(k) +
+                                               " columns exceeds the maximum of " +
+                                               std::to_string(si::kNoAllocMaxCols) + " held by the static scratch");
+    si::normalize_signs_noalloc_dev(ex, coords, static_cast<int64_t>(n), static_cast<int>(k));
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
+  });
+}
+
 si_status si_scale_and_add_noise(si_ctx* ctx, const double* coords, uint64_t n, uint32_t k, uint64_t seed,
                                  float* out) {
   return guarded(ctx, [&] {

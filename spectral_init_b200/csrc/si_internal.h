@@ -195,6 +195,12 @@ template <class XT>
 void lobpcg_update_dev(const Exec& ex, const LobpcgBlocks<XT>& b, const LobpcgCtrl* ctrl, int ld, int64_t n,
                        int init_mode);
 
+// ---- noalloc.cu -----------------------------------------------------------------
+// Sign normalisation of a contiguous f64 block [n x k] with all temporaries in
+// a static device array (no allocation); k <= kNoAllocMaxCols.
+constexpr int kNoAllocMaxCols = 64;
+void normalize_signs_noalloc_dev(const Exec& ex, double* x, int64_t n, int k);
+
 // ---- dense_evd.cu ---------------------------------------------------------------
 // k smallest eigenpairs of the dense symmetric matrix of an operator
 // (explicit CSR or implicit-diagonal form).  evals host [k], evecs device
