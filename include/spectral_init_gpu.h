@@ -87,6 +87,8 @@ typedef struct si_report {
   int32_t n_components_graph;/* connected components found                          */
   int32_t fp32_iterations;   /* iterations run in the f32 phase (mixed mode)       */
   int32_t spmm_calls;        /* operator applications                              */
+  int32_t learned_start;     /* 1 when the accepted solve started from the learned block */
+  int32_t reserved1;
   double max_residual;       /* level-gate residual (src/metrics.rs:73-92)         */
   double solve_ms;           /* device time of the eigensolve                      */
   double eigenvalues[16];    /* first min(k,16) eigenvalues of the accepted level  */
@@ -239,6 +241,46 @@ si_status si_normalize_signs_noalloc(si_ctx* ctx, double* coords, uint64_t n, ui
  * [n x k]: max-|.| scaled to 10, plus N(0, 1e-4) noise from `seed`. */
 si_status si_scale_and_add_noise(si_ctx* ctx, const double* coords, uint64_t n, uint32_t k,
                                  uint64_t seed, float* out);
+
+/* ---- learned warm start (no counterpart in the crate) ----------------------- */
+
+/* The warm-start network: 3 message-passing layers (hidden width 64, bf16
+ * weights, f32 accumulation) over the normalised adjacency, fed with the
+ * square-root degree and 4 Chebyshev-filtered random probes per node, predicting
+ * a 16-column block whose first k columns start LOBPCG.  Its parameters are a
+ * flat f32 vector of si_model_param_count() values. */
+typedef struct si_model si_model;
+uint64_t si_model_param_count(void);
+/* New model with He-initialised weights from `seed` on the context's device. */
+si_status si_model_create(si_ctx* ctx, uint64_t seed, si_model** out);
+void si_model_destroy(si_model* model);
+si_status si_model_set_params(si_ctx* ctx, si_model* model, const float* params);  /* HOST [count] */
+si_status si_model_get_params(si_ctx* ctx, si_model* model, float* params);        /* HOST [count] */
+/* One Adam step (lr) of the subspace-projection loss on one graph.  op: DEVICE
+ * Laplacian operator with f32 values; sqrt_deg: DEVICE [n]; target: DEVICE f64
+ * [n x k] orthonormal eigenvectors (k <= 16); seed draws the random probes.
+ * *loss (HOST) receives the loss before the step. */
+si_status si_model_train_step(si_ctx* ctx, si_model* model, const si_operator* op, const double* sqrt_deg,
+                              const double* target, uint32_t k, uint64_t seed, float lr, double* loss);
+/* Loss and gradient (HOST [count]) without an update.  features: DEVICE f32
+ * [n x 5] replacing the computed features, or NULL. */
+si_status si_model_gradient(si_ctx* ctx, si_model* model, const si_operator* op, const double* sqrt_deg,
+                            const float* features, const double* target, uint32_t k, uint64_t seed,
+                            double* loss, float* grad);
+/* Prediction Y: DEVICE f32 [n x 16].  features as for si_model_gradient. */
+si_status si_model_predict(si_ctx* ctx, si_model* model, const si_operator* op, const double* sqrt_deg,
+                           const float* features, uint64_t seed, float* out);
+/* Model used by solves whose si_config.warm_start is SI_WARM_START_LEARNED
+ * (NULL detaches).  The model must outlive its use by the context. */
+si_status si_ctx_set_model(si_ctx* ctx, si_model* model);
+
+/* Tensor-core building block of the warm-start network: C = A * B^T on the
+ * DEVICE, A [m x k] and B [n x k] row-major bf16 (pitches lda, ldb in elements,
+ * multiples of 8, 16-byte aligned), C [m x n] f32 with pitch ldc (multiple of 8;
+ * == n when k_splits > 1).  n must be 16, 64 or 128.  k_splits > 1 splits the
+ * k dimension across CTAs (for tall-skinny weight gradients). */
+si_status si_gemm_bf16_nt(si_ctx* ctx, uint64_t m, uint32_t n, uint64_t k, const void* a, uint64_t lda,
+                          const void* b, uint64_t ldb, float* c, uint64_t ldc, uint32_t k_splits);
 
 #ifdef __cplusplus
 }

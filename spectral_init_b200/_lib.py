@@ -40,6 +40,7 @@ class SiReport(C.Structure):
     _fields_ = [
         ("level", C.c_int32), ("iterations", C.c_int32), ("restarts", C.c_int32),
         ("n_components_graph", C.c_int32), ("fp32_iterations", C.c_int32), ("spmm_calls", C.c_int32),
+        ("learned_start", C.c_int32), ("reserved1", C.c_int32),
         ("max_residual", C.c_double), ("solve_ms", C.c_double), ("eigenvalues", C.c_double * 16),
     ]
 
@@ -91,6 +92,19 @@ _SIGNATURES = {
     "si_normalize_signs": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32]),
     "si_normalize_signs_noalloc": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32]),
     "si_scale_and_add_noise": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32, C.c_uint64, vp]),
+    "si_model_param_count": (C.c_uint64, []),
+    "si_model_create": (C.c_int, [vp, C.c_uint64, C.POINTER(vp)]),
+    "si_model_destroy": (None, [vp]),
+    "si_model_set_params": (C.c_int, [vp, vp, vp]),
+    "si_model_get_params": (C.c_int, [vp, vp, vp]),
+    "si_model_train_step": (C.c_int, [vp, vp, C.POINTER(SiOperator), vp, vp, C.c_uint32, C.c_uint64, C.c_float,
+                                      C.POINTER(C.c_double)]),
+    "si_model_gradient": (C.c_int, [vp, vp, C.POINTER(SiOperator), vp, vp, vp, C.c_uint32, C.c_uint64,
+                                    C.POINTER(C.c_double), vp]),
+    "si_model_predict": (C.c_int, [vp, vp, C.POINTER(SiOperator), vp, vp, C.c_uint64, vp]),
+    "si_ctx_set_model": (C.c_int, [vp, vp]),
+    "si_gemm_bf16_nt": (C.c_int, [vp, C.c_uint64, C.c_uint32, C.c_uint64, vp, C.c_uint64, vp, C.c_uint64, vp,
+                                  C.c_uint64, C.c_uint32]),
 }
 
 _lib = None

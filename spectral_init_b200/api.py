@@ -121,11 +121,13 @@ class Report:
     max_residual: float = 0.0
     solve_ms: float = 0.0
     eigenvalues: list = field(default_factory=list)
+    learned_start: int = 0
 
     @staticmethod
     def from_c(r: SiReport, k: int) -> "Report":
         return Report(r.level, r.iterations, r.restarts, r.n_components_graph, r.fp32_iterations, r.spmm_calls,
-                      r.max_residual, r.solve_ms, [r.eigenvalues[i] for i in range(min(k, 16))])
+                      r.max_residual, r.solve_ms, [r.eigenvalues[i] for i in range(min(k, 16))],
+                      r.learned_start)
 
 
 # ---- context -------------------------------------------------------------------------

@@ -8,15 +8,24 @@
 #include <string>
 #include <vector>
 
+#include "mpnn.h"
 #include "pipeline.h"
 
 std::atomic<uint64_t> si::g_kernel_launches{0};
+
+struct si_model {
+  int device = 0;
+  si::MpnnModel m;
+  si::MpnnActs acts;
+  si::GemmWorkspace ws;
+};
 
 struct si_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   int sms = 148;
   std::string last_error;
+  si_model* model = nullptr;  // learned warm start
   si::Exec ex() const {
     si::Exec e;
     e.stream = stream;
@@ -76,7 +85,20 @@ si::OpDev op_of(const si_operator* op) {
   return d;
 }
 
-si::SolverConfig solver_cfg(const si_config* cfg) {
+// Learned start of a solve: features, forward pass, first k predicted columns.
+bool learned_block(si_model* model, const si::Exec& ex, const si::OpDev& op, const double* sqrt_deg, int k,
+                   uint64_t seed, double* x, int ld) {
+  if (op.v32 == nullptr || sqrt_deg == nullptr || k > si::kMpnnOut) return false;
+  si::mpnn_features(ex, op, sqrt_deg, seed, nullptr, model->acts);
+  si::mpnn_forward(ex, model->m, op, model->acts, model->ws);
+  std::vector<int> cols(k);
+  for (int c = 0; c < k; ++c) cols[c] = c;
+  si::gather_columns_dev<float, double>(ex, model->acts.y.get(), si::kMpnnOut, x, ld, op.n, cols);
+  si::gemm_check(ex, model->ws);
+  return true;
+}
+
+si::SolverConfig solver_cfg(si_ctx* ctx, const si_config* cfg) {
   si_config c;
   if (cfg) c = *cfg; else si_config_default(&c);
   si::SolverConfig s;
@@ -95,6 +117,13 @@ si::SolverConfig solver_cfg(const si_config* cfg) {
              SI_INVALID_ARGUMENT, "config: unknown compute_mode");
   SI_REQUIRE(c.warm_start == SI_WARM_START_RANDOM || c.warm_start == SI_WARM_START_LEARNED, SI_INVALID_ARGUMENT,
              "config: unknown warm_start");
+  if (c.warm_start == SI_WARM_START_LEARNED) {
+    SI_REQUIRE(ctx->model != nullptr, SI_INVALID_ARGUMENT,
+               "config: warm_start LEARNED needs a model attached with si_ctx_set_model");
+    si_model* model = ctx->model;
+    s.learned_start = [model](const si::Exec& ex, const si::OpDev& op, const double* sq, int k, uint64_t seed,
+                              double* x, int ld) { return learned_block(model, ex, op, sq, k, seed, x, ld); };
+  }
   return s;
 }
 
@@ -107,6 +136,7 @@ void fill_report(si_report* rep, const si::SolverStats& st, int ncomp, const std
   rep->n_components_graph = ncomp;
   rep->fp32_iterations = st.fp32_iterations;
   rep->spmm_calls = st.spmm_calls;
+  rep->learned_start = st.learned_used;
   rep->max_residual = st.max_residual;
   rep->solve_ms = ms;
   for (size_t i = 0; i < vals.size() && i < 16; ++i) rep->eigenvalues[i] = vals[i];
@@ -141,6 +171,12 @@ struct HostCsr64 {
     op = si::op_from_csr64(indptr.get(), indices.get(), data.get(), n, nnz);
   }
 };
+
+si_model* checked_model(si_ctx* ctx, si_model* model) {
+  SI_REQUIRE(model != nullptr, SI_INVALID_ARGUMENT, "model is null");
+  SI_REQUIRE(model->device == ctx->device, SI_INVALID_ARGUMENT, "model lives on another device");
+  return model;
+}
 
 }  // namespace
 
@@ -218,7 +254,7 @@ si_status si_spectral_init_device(si_ctx* ctx, const si_csr_f32* graph, uint32_t
     const si::Exec ex = ctx->ex();
     si::GraphDev g = graph_of(graph);
     si::PipelineConfig pc;
-    pc.solver = solver_cfg(cfg);
+    pc.solver = solver_cfg(ctx, cfg);
     pc.compute_mode = cfg ? cfg->compute_mode : SI_COMPUTE_PYTHON_COMPAT;
     SI_REQUIRE(out != nullptr || g.n == 0 || n_components == 0, SI_INVALID_ARGUMENT, "out is null");
     si::PipelineReport rep;
@@ -274,7 +310,7 @@ si_status si_spectral_init(si_ctx* ctx, const si_csr_f32* graph, uint32_t n_comp
     si_csr_f32 dg{static_cast<uint64_t>(n), static_cast<uint64_t>(nnz), ip.get(), ix.get(), dv.get()};
     si::GraphDev g = graph_of(&dg);
     si::PipelineConfig pc;
-    pc.solver = solver_cfg(cfg);
+    pc.solver = solver_cfg(ctx, cfg);
     pc.compute_mode = cfg ? cfg->compute_mode : SI_COMPUTE_PYTHON_COMPAT;
     si::PipelineReport rep;
     cudaEvent_t e0, e1;
@@ -388,7 +424,7 @@ si_status si_solve_eigenproblem(si_ctx* ctx, const si_operator* op, uint32_t n_c
     si::OpDev o = op_of(op);
     SI_REQUIRE(n_components >= 1 && static_cast<int64_t>(n_components) < o.n, SI_INVALID_ARGUMENT,
                "need 1 <= n_components < n");
-    si::SolverConfig sc = solver_cfg(cfg);
+    si::SolverConfig sc = solver_cfg(ctx, cfg);
     si::EigenResult r;
     si::SolverStats st;
     si::solve_eigenproblem_dev(ex, o, static_cast<int>(n_components), seed, sqrt_deg, sc, r, st);
@@ -414,7 +450,7 @@ si_status si_solve_eigenproblem_host(si_ctx* ctx, const si_csr_f64* laplacian, u
     std::vector<double> ones(n, 1.0);
     si::DevBuf<double> sq(n, ex.stream);
     SI_CUDA(cudaMemcpyAsync(sq.get(), ones.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ex.stream));
-    si::SolverConfig sc = solver_cfg(cfg);
+    si::SolverConfig sc = solver_cfg(ctx, cfg);
     si::EigenResult r;
     si::SolverStats st;
     si::solve_eigenproblem_dev(ex, L.op, static_cast<int>(n_components), seed, sq.get(), sc, r, st);
@@ -437,7 +473,7 @@ si_status si_lobpcg_solve_host(si_ctx* ctx, const si_csr_f64* op, uint32_t n_com
     SI_REQUIRE(sqrt_deg != nullptr, SI_INVALID_ARGUMENT, "sqrt_deg is null");
     si::DevBuf<double> sq(n, ex.stream);
     SI_CUDA(cudaMemcpyAsync(sq.get(), sqrt_deg, sizeof(double) * n, cudaMemcpyHostToDevice, ex.stream));
-    si::SolverConfig sc = solver_cfg(cfg);
+    si::SolverConfig sc = solver_cfg(ctx, cfg);
     si::EigenResult r;
     si::SolverStats st;
     const bool ok = si::lobpcg_solve_dev(ex, L.op, static_cast<int>(n_components), seed, regularize != 0, sq.get(),
@@ -508,6 +544,128 @@ si_status si_normalize_signs_noalloc(si_ctx* ctx, double* coords, uint64_t n, ui
                                                std::to_string(si::kNoAllocMaxCols) + " held by the static scratch");
     si::normalize_signs_noalloc_dev(ex, coords, static_cast<int64_t>(n), static_cast<int>(k));
     SI_CUDA(cudaStreamSynchronize(ex.stream));
+  });
+}
+
+uint64_t si_model_param_count(void) { return static_cast<uint64_t>(si::mpnn_param_count()); }
+
+si_status si_model_create(si_ctx* ctx, uint64_t seed, si_model** out) {
+  if (out == nullptr) return SI_INVALID_ARGUMENT;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    si_model* m = new si_model();
+    m->device = ctx->device;
+    try {
+      m->m.init(ctx->ex(), seed);
+      SI_CUDA(cudaStreamSynchronize(ctx->stream));
+    } catch (...) {
+      delete m;
+      throw;
+    }
+    *out = m;
+  });
+}
+
+void si_model_destroy(si_model* model) {
+  if (model == nullptr) return;
+  cudaSetDevice(model->device);
+  cudaDeviceSynchronize();
+  delete model;
+}
+
+si_status si_model_set_params(si_ctx* ctx, si_model* model, const float* params) {
+  return guarded(ctx, [&] {
+    SI_REQUIRE(params != nullptr, SI_INVALID_ARGUMENT, "params is null");
+    checked_model(ctx, model)->m.set(ctx->ex(), params);
+  });
+}
+
+si_status si_model_get_params(si_ctx* ctx, si_model* model, float* params) {
+  return guarded(ctx, [&] {
+    SI_REQUIRE(params != nullptr, SI_INVALID_ARGUMENT, "params is null");
+    checked_model(ctx, model)->m.get(ctx->ex(), params);
+  });
+}
+
+si_status si_model_train_step(si_ctx* ctx, si_model* model, const si_operator* op, const double* sqrt_deg,
+                              const double* target, uint32_t k, uint64_t seed, float lr, double* loss) {
+  return guarded(ctx, [&] {
+    si_model* m = checked_model(ctx, model);
+    const si::Exec ex = ctx->ex();
+    si::OpDev o = op_of(op);
+    SI_REQUIRE(o.n > 0 && o.v32 != nullptr && target != nullptr && sqrt_deg != nullptr, SI_INVALID_ARGUMENT,
+               "train_step: needs a non-empty operator with f32 values, sqrt_deg and target");
+    si::mpnn_features(ex, o, sqrt_deg, seed, nullptr, m->acts);
+    si::mpnn_forward(ex, m->m, o, m->acts, m->ws);
+    const double l = si::mpnn_loss_backward(ex, m->m, o, m->acts, target, static_cast<int>(k), static_cast<int>(k),
+                                            m->ws);
+    si::mpnn_adam(ex, m->m, lr);
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
+    if (loss) *loss = l;
+  });
+}
+
+si_status si_model_gradient(si_ctx* ctx, si_model* model, const si_operator* op, const double* sqrt_deg,
+                            const float* features, const double* target, uint32_t k, uint64_t seed, double* loss,
+                            float* grad) {
+  return guarded(ctx, [&] {
+    si_model* m = checked_model(ctx, model);
+    const si::Exec ex = ctx->ex();
+    si::OpDev o = op_of(op);
+    SI_REQUIRE(o.n > 0 && o.v32 != nullptr && target != nullptr, SI_INVALID_ARGUMENT,
+               "gradient: needs a non-empty operator with f32 values and a target");
+    si::mpnn_features(ex, o, sqrt_deg, seed, features, m->acts);
+    si::mpnn_forward(ex, m->m, o, m->acts, m->ws);
+    const double l = si::mpnn_loss_backward(ex, m->m, o, m->acts, target, static_cast<int>(k), static_cast<int>(k),
+                                            m->ws);
+    if (grad != nullptr)
+      SI_CUDA(cudaMemcpyAsync(grad, m->m.grad.get(), sizeof(float) * m->m.grad.size(), cudaMemcpyDeviceToHost,
+                              ex.stream));
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
+    if (loss) *loss = l;
+  });
+}
+
+si_status si_model_predict(si_ctx* ctx, si_model* model, const si_operator* op, const double* sqrt_deg,
+                           const float* features, uint64_t seed, float* out) {
+  return guarded(ctx, [&] {
+    si_model* m = checked_model(ctx, model);
+    const si::Exec ex = ctx->ex();
+    si::OpDev o = op_of(op);
+    SI_REQUIRE(o.n > 0 && o.v32 != nullptr && out != nullptr, SI_INVALID_ARGUMENT,
+               "predict: needs a non-empty operator with f32 values and an output");
+    si::mpnn_features(ex, o, sqrt_deg, seed, features, m->acts);
+    si::mpnn_forward(ex, m->m, o, m->acts, m->ws);
+    SI_CUDA(cudaMemcpyAsync(out, m->acts.y.get(), sizeof(float) * o.n * si::kMpnnOut, cudaMemcpyDeviceToDevice,
+                            ex.stream));
+    si::gemm_check(ex, m->ws);
+  });
+}
+
+si_status si_ctx_set_model(si_ctx* ctx, si_model* model) {
+  return guarded(ctx, [&] {
+    if (model != nullptr) checked_model(ctx, model);
+    ctx->model = model;
+  });
+}
+
+si_status si_gemm_bf16_nt(si_ctx* ctx, uint64_t m, uint32_t n, uint64_t k, const void* a, uint64_t lda,
+                          const void* b, uint64_t ldb, float* c, uint64_t ldc, uint32_t k_splits) {
+  return guarded(ctx, [&] {
+    const si::Exec ex = ctx->ex();
+    if (m == 0) return;
+    if (a == nullptr || b == nullptr || c == nullptr)
+      throw si::Error(SI_INVALID_ARGUMENT, "gemm_bf16_nt: null operand");
+    si::GemmEpilogue ep;
+    ep.mode = si::GEMM_STORE_F32;
+    ep.out_f32 = c;
+    ep.ldo = static_cast<int64_t>(ldc);
+    si::GemmWorkspace ws;
+    si::gemm_bf16_nt(ex, static_cast<int64_t>(m), static_cast<int>(n), static_cast<int64_t>(k),
+                     static_cast<const __nv_bfloat16*>(a), static_cast<int64_t>(lda),
+                     static_cast<const __nv_bfloat16*>(b), static_cast<int64_t>(ldb), ep,
+                     static_cast<int>(k_splits), ws);
+    si::gemm_check(ex, ws);
   });
 }
 

@@ -305,7 +305,20 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
 
   LobpcgState<double> s;
   s.alloc(ex, n, m, ld);
-  if (cfg.warm_start != nullptr) {
+  bool learned = false;
+  if (cfg.learned_start && sqrt_deg != nullptr && !regularize) {
+    // predicted columns [0, k) over a random block (guard columns), the
+    // trivial eigenvector injected exactly in column 0
+    fill_normal_dev<double>(ex, s.X.get(), n, m, ld, seed, 1);
+    SI_CUDA(cudaMemsetAsync(s.R.get(), 0, sizeof(double) * n * ld, ex.stream));
+    learned = cfg.learned_start(ex, op, sqrt_deg, k, seed, s.R.get(), ld);
+    if (learned) {
+      std::vector<int> cols(k);
+      std::iota(cols.begin(), cols.end(), 0);
+      gather_columns_dev<double, double>(ex, s.R.get(), ld, s.X.get(), ld, n, cols);
+    }
+    set_column_normalized_dev<double>(ex, s.gw, s.X.get(), ld, n, sqrt_deg);
+  } else if (cfg.warm_start != nullptr) {
     SI_CUDA(cudaMemsetAsync(s.X.get(), 0, sizeof(double) * n * ld, ex.stream));
     std::vector<int> cols(std::min(m, cfg.warm_start_ld));
     std::iota(cols.begin(), cols.end(), 0);
@@ -326,7 +339,8 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
     LobpcgState<float> s32;
     s32.alloc(ex, n, m, ld);
     gather_columns_dev<double, float>(ex, s.X.get(), ld, s32.X.get(), ld, n, all_cols);
-    if (n >= CHEB_MIN_N) chebyshev_start<float>(ex, A, s32, true, st.spmm_calls);
+    if (n >= CHEB_MIN_N && (!learned || cfg.learned_chebyshev))
+      chebyshev_start<float>(ex, A, s32, true, st.spmm_calls);
     const double switch_tol = cfg.mixed_switch_tol > 0.0 ? cfg.mixed_switch_tol : 1e-4;
     const int maxiter32 = static_cast<int>(std::min<int64_t>(5 * n, cfg.max_iterations > 0 ? cfg.max_iterations
                                                                                            : LOBPCG_RESTART_MAXITER_CAP));
@@ -338,7 +352,7 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
     } else {
       gather_columns_dev<float, double>(ex, s32.X.get(), ld, s.X.get(), ld, n, all_cols);
     }
-  } else if (n >= CHEB_MIN_N) {
+  } else if (n >= CHEB_MIN_N && (!learned || cfg.learned_chebyshev)) {
     chebyshev_start<double>(ex, A, s, false, st.spmm_calls);
   }
 
@@ -357,6 +371,14 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
     if (!accept) {
       accept = true;
       for (int c = 0; c < k; ++c) accept = accept && (o.best_rnorm[c] < LOBPCG_ACCEPT_TOL);
+    }
+    if (!accept && learned && restart == 0) {
+      // the learned block stalled: start over from the random block
+      fill_normal_dev<double>(ex, s.X.get(), n, m, ld, seed, 1);
+      set_column_normalized_dev<double>(ex, s.gw, s.X.get(), ld, n, sqrt_deg);
+      if (n >= CHEB_MIN_N) chebyshev_start<double>(ex, A, s, false, st.spmm_calls);
+      learned = false;
+      continue;
     }
     if (!accept) {
       if (restart < MAX_WARM_RESTARTS) {
@@ -379,6 +401,7 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
       gather_columns_dev<double, double>(ex, s.X.get(), ld, out.vecs.get(), k, n,
                                          std::vector<int>(all_cols.begin(), all_cols.begin() + k));
       st.restarts = restart_count;
+      st.learned_used = learned ? 1 : 0;
       return true;
     }
     ++restart_count;

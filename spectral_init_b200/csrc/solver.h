@@ -1,6 +1,7 @@
 // Eigensolver drivers (host C++ orchestrating the device kernels).
 #pragma once
 
+#include <functional>
 #include <vector>
 
 #include "si_internal.h"
@@ -20,9 +21,16 @@ struct SolverConfig {
   // warm start: optional device block [n x ld_ws] (f64) replacing the random start
   const double* warm_start = nullptr;
   int warm_start_ld = 0;
+  // learned warm start: writes a predicted block into columns [0, k) of the
+  // device f64 block x [n x ld]; false falls back to the random start
+  std::function<bool(const Exec& ex, const OpDev& op, const double* sqrt_deg, int k, uint64_t seed, double* x,
+                     int ld)>
+      learned_start;
+  bool learned_chebyshev = false;  // also apply the Chebyshev start filter to the learned block
 };
 
 struct SolverStats {
+  int learned_used = 0;  // the accepted solve started from the learned block
   int level = -1;
   int iterations = 0;
   int restarts = 0;

@@ -1,0 +1,125 @@
+"""Learned warm start on the device: gradients against the CPU oracle, training,
+prediction, and the solve that starts from the prediction.
+
+The gradient check feeds the same features, parameters and operator to the
+device passes (bf16 tcgen05 GEMMs, f32 accumulation) and to the numpy oracle
+with the same bf16 rounding points; what remains is summation order and the
+rare bf16 rounding flip that it causes, so the loss must agree to 1e-3
+relative and every parameter block's gradient to 2e-2 in relative L2 norm.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import load_graph
+from oracle import mpnn_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(ctx, dataset="blobs_connected_2000", k=3):
+    import torch
+    from spectral_init_b200.warm_start import DeviceLaplacian
+    g = load_graph(dataset)
+    lap = DeviceLaplacian(g, ctx=ctx)
+    n = lap.n
+    ip = lap.indptr.cpu().numpy()
+    ix = lap.indices.cpu().numpy()
+    v64 = lap.v64[:lap.nnz].cpu().numpy()
+    v32 = lap.v32[:lap.nnz].cpu().numpy()
+    L = sp.identity(n) + sp.csr_matrix((v64, ix, ip), shape=(n, n))
+    _, vecs = np.linalg.eigh(L.toarray())
+    target = torch.from_numpy(np.ascontiguousarray(vecs[:, :k])).to("cuda:0")
+    ahat = M.ahat_from_values(ip, ix, v32, n)
+    return lap, target, vecs[:, :k], ahat
+
+
+def _blocks(vec):
+    layers_idx, o = [], 0
+    for _ in range(M.LAYERS):
+        layers_idx.append((o, o + M.HIDDEN * M.CAT))
+        o += M.HIDDEN * M.CAT
+        layers_idx.append((o, o + M.HIDDEN))
+        o += M.HIDDEN
+    layers_idx.append((o, o + M.OUT * M.CAT))
+    o += M.OUT * M.CAT
+    layers_idx.append((o, o + M.OUT))
+    return [vec[a:b] for a, b in layers_idx]
+
+
+@pytest.mark.parametrize("model_seed", [3, 11])
+def test_gradient_matches_cpu_oracle(gpu_ctx, model_seed):
+    import torch
+    from spectral_init_b200.warm_start import WarmStartModel
+    lap, target, v, ahat = _setup(gpu_ctx)
+    rng = np.random.default_rng(model_seed)
+    feats = rng.standard_normal((lap.n, M.FEATURES)).astype(np.float32)
+    model = WarmStartModel(model_seed, ctx=gpu_ctx)
+    params = model.get_params()
+    loss_gpu, grad_gpu = model.gradient(lap, target, features=torch.from_numpy(feats).to("cuda:0"))
+    loss_cpu, grad_cpu = M.loss_and_grad(params, ahat, feats, v, 3, rounding=True)
+    assert abs(loss_gpu - loss_cpu) <= 1e-3 * abs(loss_cpu), (loss_gpu, loss_cpu)
+    for i, (g, c) in enumerate(zip(_blocks(grad_gpu.astype(np.float64)), _blocks(grad_cpu))):
+        nrm = np.linalg.norm(c)
+        assert np.linalg.norm(g - c) <= 2e-2 * max(nrm, 1e-12), (i, np.linalg.norm(g - c), nrm)
+    model.close()
+
+
+def test_prediction_matches_oracle_forward(gpu_ctx):
+    import torch
+    from spectral_init_b200.warm_start import WarmStartModel
+    lap, _, _, ahat = _setup(gpu_ctx)
+    feats = np.random.default_rng(5).standard_normal((lap.n, M.FEATURES)).astype(np.float32)
+    model = WarmStartModel(7, ctx=gpu_ctx)
+    y = model.predict(lap, features=torch.from_numpy(feats).to("cuda:0")).cpu().numpy()
+    y_cpu, _ = M.forward(model.get_params(), ahat, feats, rounding=True)
+    err = np.abs(y - y_cpu).max()
+    assert err <= 2e-2 * np.abs(y_cpu).max(), err
+    # computed features: deterministic for a seed
+    y1 = model.predict(lap, seed=9)
+    y2 = model.predict(lap, seed=9)
+    assert torch.equal(y1, y2)
+    model.close()
+
+
+def test_training_reduces_the_subspace_loss(gpu_ctx):
+    from spectral_init_b200.warm_start import WarmStartModel
+    lap, target, _, _ = _setup(gpu_ctx)
+    model = WarmStartModel(1, ctx=gpu_ctx)
+    losses = [model.train_step(lap, target, seed=4, lr=3e-3) for _ in range(60)]
+    assert all(np.isfinite(losses))
+    assert 0.0 <= min(losses) <= 1.0
+    assert np.mean(losses[-5:]) < 0.8 * np.mean(losses[:5]), (losses[:5], losses[-5:])
+    model.close()
+
+
+def test_params_round_trip_and_file_format(gpu_ctx, tmp_path):
+    from spectral_init_b200.warm_start import WarmStartModel, load_params, param_count
+    model = WarmStartModel(2, ctx=gpu_ctx)
+    p = model.get_params()
+    assert p.size == param_count() == M.param_count()
+    model.save(tmp_path / "w.bin")
+    q = load_params(tmp_path / "w.bin")
+    assert np.array_equal(p, q)
+    other = WarmStartModel(99, ctx=gpu_ctx, params=q)
+    assert np.array_equal(other.get_params(), p)
+    model.close()
+    other.close()
+
+
+def test_learned_solve_passes_the_fp64_gate(gpu_ctx):
+    """A solve started from the network's block (random weights: a poor start)
+    still ends at the FP64 residual gate, through the fallback if needed."""
+    import spectral_init_b200 as si
+    from spectral_init_b200.warm_start import WarmStartModel
+    g = load_graph("blobs_connected_2000")
+    model = WarmStartModel(5, ctx=gpu_ctx)
+    model.attach()
+    cfg = si.SpectralInitConfig(precision=si.Precision.MIXED, warm_start=si.WarmStart.LEARNED)
+    out, rep = si.spectral_init(g, 2, 42, config=cfg, ctx=gpu_ctx, return_report=True)
+    assert out.shape == (g.shape[0], 2)
+    assert rep.max_residual < 1e-5
+    model.detach()
+    with pytest.raises(si.InvalidArgument):
+        si.spectral_init(g, 2, 42, config=cfg, ctx=gpu_ctx)
+    model.close()
