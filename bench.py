@@ -55,6 +55,7 @@ def parse_args():
     p.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU LOBPCG per baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
     p.add_argument("--spmm-profile", action="store_true", help="SpMM launches only (n=--n), for ncu")
     p.add_argument("--spmm-prec", choices=["both", "f64", "f32"], default="both",
                    help="with --spmm-profile: which SpMM precision to run")
@@ -251,10 +252,21 @@ def run_ours(a):
     # ---- eigensolves ------------------------------------------------------------------------
     k = a.nc + 1
 
-    def solve(precision: int):
+    # learned warm start: the committed network weights, when present
+    model = None
+    if not a.no_learned:
+        from spectral_init_b200.warm_start import WEIGHTS_PATH, WarmStartModel
+        if WEIGHTS_PATH.exists():
+            model = WarmStartModel.load(ctx=ctx)
+            model.attach()
+    legs = [(0, 0, "fp64"), (1, 0, "mixed")] + ([(1, 1, "learned")] if model is not None else [])
+    head = legs[-1][2]
+
+    def solve(precision: int, warm: int = 0):
         cfg = SiConfig()
         lib.si_config_default(C.byref(cfg))
         cfg.precision = precision
+        cfg.warm_start = warm
         vals = (C.c_double * k)()
         vecs = torch.empty(n, k, dtype=torch.float64, device=dev)
         level = C.c_int32(-1)
@@ -271,28 +283,29 @@ def run_ours(a):
 
     if a.profile_solve:
         out = {}
-        for prec, name in ((0, "fp64"), (1, "mixed")):
-            solve(prec)
-            ms, vals, _, level, rep = solve(prec)
-            out[name] = {"ms": ms, "iterations": rep.iterations, "level": level, "max_residual": rep.max_residual}
+        for prec, warm, name in legs:
+            solve(prec, warm)
+            ms, vals, _, level, rep = solve(prec, warm)
+            out[name] = {"ms": ms, "iterations": rep.iterations, "level": level, "max_residual": rep.max_residual,
+                         "learned_start": rep.learned_start}
         print(json.dumps({"profile_solve": True, "n": n, "nnz": nnz, **out}))
         return
 
     results = {}
     clocks = None
     launches_per_step = None
-    for prec, name in ((0, "fp64"), (1, "mixed")):
+    for prec, warm, name in legs:
         for _ in range(a.warmup):
-            solve(prec)
+            solve(prec, warm)
         barrier()
         torch.cuda.synchronize()
-        sampler = ClockSampler(local) if name == "mixed" else None
+        sampler = ClockSampler(local) if name == head else None
         if sampler:
             sampler.start()
         l0 = lib.si_kernel_launches()
         times, last = [], None
         for _ in range(a.steps):
-            ms, vals, vecs, level, rep = solve(prec)
+            ms, vals, vecs, level, rep = solve(prec, warm)
             times.append(ms)
             last = (vals, vecs, level, rep)
         torch.cuda.synchronize()
@@ -304,14 +317,15 @@ def run_ours(a):
         vals, vecs, level, rep = last
         results[name] = {"ms": ms_mean, "ms_all": times, "eigenvalues": vals, "level": level,
                          "iterations": rep.iterations, "fp32_iterations": rep.fp32_iterations,
-                         "restarts": rep.restarts, "max_residual": rep.max_residual, "vecs": vecs}
+                         "restarts": rep.restarts, "max_residual": rep.max_residual,
+                         "learned_start": rep.learned_start, "vecs": vecs}
 
     # agreement of the two solves: largest principal-angle sine and eigenvalue differences
     qa, _ = torch.linalg.qr(results["fp64"]["vecs"])
-    qb, _ = torch.linalg.qr(results["mixed"]["vecs"])
+    qb, _ = torch.linalg.qr(results[head]["vecs"])
     sin_theta = float(torch.linalg.matrix_norm(qb - qa @ (qa.T @ qb), ord=2))
     ev64 = np.array(results["fp64"]["eigenvalues"])
-    evm = np.array(results["mixed"]["eigenvalues"])
+    evm = np.array(results[head]["eigenvalues"])
     ev_rel = float(np.max(np.abs(evm - ev64) / np.maximum(np.abs(ev64), 1e-300)))
 
     # ---- end to end through the C ABI with host buffers ----------------------------------------
@@ -328,6 +342,7 @@ def run_ours(a):
         cfg = SiConfig()
         lib.si_config_default(C.byref(cfg))
         cfg.precision = 1
+        cfg.warm_start = 1 if head == "learned" else 0
         rep = SiReport()
 
         def call():
@@ -363,7 +378,7 @@ def run_ours(a):
             traffic = t["dram_bytes_per_algorithmic_byte_f32"] * bytes32
     if rank != 0:
         return
-    value_s = results["mixed"]["ms"] / 1e3
+    value_s = results[head]["ms"] / 1e3
     line = {
         "metric": METRIC,
         "value": value_s,
@@ -372,7 +387,7 @@ def run_ours(a):
         "n_gpus": world,
         "steps": a.steps,
         "warmup": a.warmup,
-        "ms_per_step": results["mixed"]["ms"],
+        "ms_per_step": results[head]["ms"],
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32 SpMM/LOBPCG bulk + f64 Gram/Rayleigh-Ritz/refinement",
@@ -381,11 +396,15 @@ def run_ours(a):
                    "block_columns": 4, "l2": "inputs larger than L2 (Laplacian "
                    f"{(nnz * 12 + (n + 1) * 8) / 1e6:.0f} MB f64 / {(nnz * 8 + (n + 1) * 8) / 1e6:.0f} MB f32)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "graph_build_s": round(t_gen, 2), "warm_start": "random (learned start not used)"},
+                   "graph_build_s": round(t_gen, 2),
+                   "warm_start": ("learned (committed network weights, trained on the n=10k-200k family)"
+                                  if head == "learned" else "random (no network weights found)")},
         "fp64": {k2: v for k2, v in results["fp64"].items() if k2 != "vecs"},
         "mixed": {k2: v for k2, v in results["mixed"].items() if k2 != "vecs"},
+        **({"learned": {k2: v for k2, v in results["learned"].items() if k2 != "vecs"}} if head == "learned" else {}),
         "speedup_mixed_vs_fp64": results["fp64"]["ms"] / results["mixed"]["ms"],
-        "mixed_vs_fp64": {"sin_theta_max": sin_theta, "eigenvalue_rel_diff_max": ev_rel},
+        "speedup_value_vs_fp64": results["fp64"]["ms"] / results[head]["ms"],
+        "value_vs_fp64": {"leg": head, "sin_theta_max": sin_theta, "eigenvalue_rel_diff_max": ev_rel},
         "spmm": {"ms_f64": ms64, "ms_f32": ms32, "gbs_f64": gbs64, "gbs_f32": gbs32,
                  "algorithmic_bytes_f64": bytes64, "algorithmic_bytes_f32": bytes32,
                  "bytes_formula": "nnz*(4 idx + s_val) + (n+1)*8 indptr + 2*n*4*s_x (x read, y written; 4 columns)"},

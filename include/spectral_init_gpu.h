@@ -74,7 +74,7 @@ typedef struct si_config {
   int32_t rsvd_oversampling; /* < 0 = crate formula (src/solvers/rsvd.rs:84-87)   */
   int32_t rsvd_nbiter;       /* <= 0 = 2 (src/solvers/rsvd.rs:123-126)           */
   int32_t max_iterations;    /* <= 0 = crate caps (300 first pass, 1000 restarts)  */
-  int32_t reserved0;
+  int32_t learned_filter;    /* 1: also apply the Chebyshev start filter to a learned block */
   double tol;                /* <= 0 = 1e-5 (src/metrics.rs:30,40)                 */
   double mixed_switch_tol;   /* mixed mode: f32 phase stops at this residual; <=0 auto */
 } si_config;

@@ -32,7 +32,7 @@ class SiConfig(C.Structure):
         ("compute_mode", C.c_int32), ("precision", C.c_int32), ("warm_start", C.c_int32),
         ("block_size", C.c_int32), ("dense_threshold", C.c_int32), ("force_level", C.c_int32),
         ("rsvd_oversampling", C.c_int32), ("rsvd_nbiter", C.c_int32), ("max_iterations", C.c_int32),
-        ("reserved0", C.c_int32), ("tol", C.c_double), ("mixed_switch_tol", C.c_double),
+        ("learned_filter", C.c_int32), ("tol", C.c_double), ("mixed_switch_tol", C.c_double),
     ]
 
 

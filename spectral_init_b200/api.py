@@ -54,6 +54,7 @@ class SpectralInitConfig:
     rsvd_oversampling: int = -1
     rsvd_nbiter: int = 0
     max_iterations: int = 0
+    learned_filter: int = 0
     tol: float = 0.0
     mixed_switch_tol: float = 0.0
 
@@ -61,7 +62,7 @@ class SpectralInitConfig:
         c = SiConfig()
         _lib.load().si_config_default(C.byref(c))
         for f in ("compute_mode", "precision", "warm_start", "block_size", "dense_threshold", "force_level",
-                  "rsvd_oversampling", "rsvd_nbiter", "max_iterations"):
+                  "rsvd_oversampling", "rsvd_nbiter", "max_iterations", "learned_filter"):
             setattr(c, f, int(getattr(self, f)))
         c.tol = float(self.tol)
         c.mixed_switch_tol = float(self.mixed_switch_tol)

@@ -111,6 +111,7 @@ si::SolverConfig solver_cfg(si_ctx* ctx, const si_config* cfg) {
   s.precision = c.precision;
   s.tol = c.tol > 0.0 ? c.tol : 1e-5;
   s.mixed_switch_tol = c.mixed_switch_tol;
+  s.learned_chebyshev = c.learned_filter != 0;
   SI_REQUIRE(c.precision == SI_PRECISION_FP64 || c.precision == SI_PRECISION_MIXED, SI_INVALID_ARGUMENT,
              "config: unknown precision");
   SI_REQUIRE(c.compute_mode == SI_COMPUTE_PYTHON_COMPAT || c.compute_mode == SI_COMPUTE_RUST_NATIVE,

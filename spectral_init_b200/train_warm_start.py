@@ -54,7 +54,7 @@ def n_components(ctx, g, n):
     return int(cnt.value)
 
 
-def solve(ctx, lap, precision, warm_start, seed=42, nc=2):
+def solve(ctx, lap, precision, warm_start, seed=42, nc=2, learned_filter=0):
     """(vecs torch f64 [n, nc+1], report) from si_solve_eigenproblem."""
     import torch
     from ._lib import SiConfig, SiReport
@@ -63,6 +63,7 @@ def solve(ctx, lap, precision, warm_start, seed=42, nc=2):
     ctx.lib.si_config_default(C.byref(cfg))
     cfg.precision = precision
     cfg.warm_start = warm_start
+    cfg.learned_filter = learned_filter
     vals = (C.c_double * k)()
     vecs = torch.empty(lap.n, k, dtype=torch.float64, device=lap.v64.device)
     level = C.c_int32(-1)
@@ -84,6 +85,8 @@ def main(argv=None):
     p.add_argument("--n-max", type=int, default=200_000)
     p.add_argument("--out", default=None)
     p.add_argument("--time-budget", type=float, default=1e9, help="stop generating after this many seconds")
+    p.add_argument("--eval-1m", action="store_true",
+                   help="also compare the starts on the held-out n=1M, k=15 benchmark graph")
     a = p.parse_args(argv)
 
     import torch
@@ -141,12 +144,29 @@ def main(argv=None):
             continue
         lap = DeviceLaplacian((g[0], g[1], g[2], n), ctx=ctx)
         row = dict(meta)
-        for name, ws in (("random", 0), ("learned", 1)):
-            solve(ctx, lap, 1, ws)
-            _, rep, level, sec = solve(ctx, lap, 1, ws)
+        for name, ws, lf in (("random", 0, 0), ("learned", 1, 0), ("learned_filtered", 1, 1)):
+            solve(ctx, lap, 1, ws, learned_filter=lf)
+            _, rep, level, sec = solve(ctx, lap, 1, ws, learned_filter=lf)
             row[name] = {"iterations": rep.iterations, "s": round(sec, 4), "level": level,
                          "residual": rep.max_residual}
         print(json.dumps({"phase": "holdout", **row}), flush=True)
+    if a.eval_1m:
+        from . import synthetic
+        n = 1_000_000
+        x = synthetic.gaussian_mixture_gpu(n, 100, 50, 42, 2.0, 0.05, device=dev)
+        idx, dist = synthetic.knn_gpu(x, 15)
+        del x
+        sigma, rho = synthetic.smooth_knn_gpu(dist, 15)
+        g = synthetic.fuzzy_graph_gpu(idx, dist, sigma, rho)
+        del idx, dist
+        lap = DeviceLaplacian((g[0], g[1], g[2], n), ctx=ctx)
+        row = {"n": n, "clusters": 100, "dims": 50, "k": 15, "center_std": 2.0, "background": 0.05}
+        for name, ws, lf in (("random", 0, 0), ("learned", 1, 0), ("learned_filtered", 1, 1)):
+            solve(ctx, lap, 1, ws, learned_filter=lf)
+            _, rep, level, sec = solve(ctx, lap, 1, ws, learned_filter=lf)
+            row[name] = {"iterations": rep.iterations, "s": round(sec, 4), "level": level,
+                         "residual": rep.max_residual, "learned_used": rep.learned_start}
+        print(json.dumps({"phase": "heldout_1m", **row}), flush=True)
     model.close()
 
 
