@@ -195,6 +195,17 @@ template <class XT>
 void lobpcg_update_dev(const Exec& ex, const LobpcgBlocks<XT>& b, const LobpcgCtrl* ctrl, int ld, int64_t n,
                        int init_mode);
 
+// ---- cg.cu -----------------------------------------------------------------------
+// Block CG on M Y = B (M symmetric positive definite, the operator with its
+// diagonal coefficient), one CG per column; returns the iterations run.
+struct CgWork {
+  DevBuf<double> r, p, q, partial;
+  DevBuf<unsigned> counter;
+  DevBuf<unsigned char> scal;
+};
+int cg_solve_block_dev(const Exec& ex, const OpDev& M, const double* b, double* y, int m, int ld, int64_t n,
+                       double rtol, int maxit, CgWork& w);
+
 // ---- noalloc.cu -----------------------------------------------------------------
 // Sign normalisation of a contiguous f64 block [n x k] with all temporaries in
 // a static device array (no allocation); k <= kNoAllocMaxCols.

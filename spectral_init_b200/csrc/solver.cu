@@ -35,6 +35,11 @@ constexpr double LOBPCG_ACCEPT_TOL = 1e-5;
 constexpr double DENSE_EVD_QUALITY_THRESHOLD = 1e-6;
 constexpr double LOBPCG_QUALITY_THRESHOLD = 1e-5;
 constexpr double RSVD_QUALITY_THRESHOLD = 1e-2;
+constexpr double SINV_SHIFT = 1e-4;                 // M = L + eps I
+constexpr double SINV_LINFA_TOL = 1e-8;
+constexpr double SINV_LOBPCG_QUALITY_THRESHOLD = 1e-6;
+constexpr double SINV_CG_RTOL = 1e-12;              // inner solve, relative residual
+constexpr int SINV_CG_MAXIT = 5000;
 constexpr int64_t DENSE_MAX_N = 8192;  // largest n the device dense EVD accepts
 
 namespace {
@@ -90,8 +95,29 @@ struct CoreOutcome {
 };
 
 template <class XT>
+CoreOutcome finish_core(const Exec& ex, LobpcgState<XT>& s, int& spmm_calls) {
+  LobpcgCtrl h;
+  SI_CUDA(cudaMemcpyAsync(&h, s.ctrl.get(), sizeof(h), cudaMemcpyDeviceToHost, ex.stream));
+  SI_CUDA(cudaStreamSynchronize(ex.stream));
+  CoreOutcome o;
+  o.status = h.status;
+  o.iterations = h.iter;
+  spmm_calls += h.iter;
+  o.best_valid = h.best_iter >= 0 && h.best_sum < DBL_MAX;
+  for (int c = 0; c < s.m; ++c) {
+    o.best_lam[c] = h.best_lam[c];
+    o.best_rnorm[c] = h.best_rnorm[c];
+  }
+  return o;
+}
+
+// apply (optional): y = Op(x) for an operator that is not a plain SpMM (the
+// shift-invert inner solve); iterations then run eagerly instead of from a
+// captured graph.
+template <class XT>
 CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int k_wanted, double tol, int maxiter,
-                        bool largest, double chol_tol, bool f32vals, int& spmm_calls) {
+                        bool largest, double chol_tol, bool f32vals, int& spmm_calls,
+                        const std::function<void(const XT*, XT*)>* apply = nullptr) {
   LobpcgCtrl h;
   std::memset(&h, 0, sizeof(h));
   h.m = s.m;
@@ -107,7 +133,8 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
   s.R.zero();
   s.AR.zero();
   Epilogue<XT> ep;
-  spmm_dev<XT>(ex, A, s.X.get(), s.AX.get(), s.ld, s.m, ep, nullptr, f32vals);
+  if (apply != nullptr) (*apply)(s.X.get(), s.AX.get());
+  else spmm_dev<XT>(ex, A, s.X.get(), s.AX.get(), s.ld, s.m, ep, nullptr, f32vals);
   ++spmm_calls;
   {
     const XT* blk[2] = {s.X.get(), s.AX.get()};
@@ -118,7 +145,8 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
   const XT* blk6[6] = {s.X.get(), s.R.get(), s.P.get(), s.AX.get(), s.AR.get(), s.AP.get()};
   auto enqueue_iterations = [&](int count) {
     for (int b = 0; b < count; ++b) {
-      spmm_dev<XT>(ex, A, s.R.get(), s.AR.get(), s.ld, s.m, ep, s.stop(), f32vals);
+      if (apply != nullptr) (*apply)(s.R.get(), s.AR.get());
+      else spmm_dev<XT>(ex, A, s.R.get(), s.AR.get(), s.ld, s.m, ep, s.stop(), f32vals);
       gram_dev<XT>(ex, s.gw, GRAM_SYM2, blk6, 3, 6, s.m, s.ld, s.n, s.gram.get(), s.stop());
       small_step_dev(ex, s.ctrl.get(), s.gram.get(), 3, SM_ITER, s.m);
       lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 0);
@@ -128,6 +156,18 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
   // replayed from a captured CUDA graph (all kernel arguments are fixed for
   // the solve, and the control state lives in device memory).
   enqueue_iterations(1);
+  if (apply != nullptr) {
+    // eager: the operator itself synchronises with the host
+    for (int launched = 1;; ++launched) {
+      int done = 0;
+      SI_CUDA(cudaMemcpyAsync(&done, s.stop(), sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
+      SI_CUDA(cudaStreamSynchronize(ex.stream));
+      if (done) break;
+      SI_REQUIRE(launched <= maxiter + 2, SI_CUDA_ERROR, "lobpcg: device loop did not terminate");
+      enqueue_iterations(1);
+    }
+    return finish_core(ex, s, spmm_calls);
+  }
   constexpr int kGraphBatch = 8;
   cudaGraphExec_t exec = nullptr;
   const uint64_t launches_before_capture = g_kernel_launches.load();
@@ -166,18 +206,7 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
     g_kernel_launches.fetch_add(per_replay);
     launched += kGraphBatch;
   }
-  SI_CUDA(cudaMemcpyAsync(&h, s.ctrl.get(), sizeof(h), cudaMemcpyDeviceToHost, ex.stream));
-  SI_CUDA(cudaStreamSynchronize(ex.stream));
-  CoreOutcome o;
-  o.status = h.status;
-  o.iterations = h.iter;
-  spmm_calls += h.iter;
-  o.best_valid = h.best_iter >= 0 && h.best_sum < DBL_MAX;
-  for (int c = 0; c < s.m; ++c) {
-    o.best_lam[c] = h.best_lam[c];
-    o.best_rnorm[c] = h.best_rnorm[c];
-  }
-  return o;
+  return finish_core(ex, s, spmm_calls);
 }
 
 // (X0 + T_8((L - cI)/e) X0) / 2 with unit columns, in place in s.X.
@@ -419,6 +448,65 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
   return true;
 }
 
+// Shift-invert LOBPCG (src/solvers/sinv.rs:106-189): LOBPCG for the k
+// largest eigenvalues mu of M^-1, M = L + eps I, then lambda = 1/mu - eps in
+// ascending order.  The crate applies M^-1 through a sparse Cholesky factor;
+// here each application is a block CG solve on the same CSR SpMM (relative
+// residual 1e-12), so the factorisation is never formed.
+bool sinv_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64_t seed, const double* sqrt_deg,
+                    const SolverConfig& cfg, EigenResult& out, SolverStats& st) {
+  RowBlocks row_blocks_;
+  OpDev op = op_in;
+  if (op.row_blocks == nullptr && op.n > 0) {
+    make_row_blocks(ex, op, row_blocks_);
+    row_blocks_.attach(op);
+  }
+  const int64_t n = op.n;
+  const int k = n_components + 1;
+  if (n_components <= 0 || k >= n || sqrt_deg == nullptr) return false;
+  SI_REQUIRE(k <= MAXM, SI_INVALID_ARGUMENT, "sinv: n_components + 1 must be <= 16");
+  const int m = choose_block(n, k, cfg.block_size);
+  const int ld = pick_ld(m);
+  LobpcgState<double> s;
+  s.alloc(ex, n, m, ld);
+  fill_normal_dev<double>(ex, s.X.get(), n, m, ld, seed, 1);
+  set_column_normalized_dev<double>(ex, s.gw, s.X.get(), ld, n, sqrt_deg);
+  OpDev M = op;
+  M.diag += SINV_SHIFT;
+  CgWork cw;
+  int inner = 0;
+  const int cg_cap = static_cast<int>(std::min<int64_t>(SINV_CG_MAXIT, 10 * n + 10));
+  const std::function<void(const double*, double*)> apply = [&](const double* x, double* y) {
+    inner += cg_solve_block_dev(ex, M, x, y, m, ld, n, SINV_CG_RTOL, cg_cap, cw);
+  };
+  const double tol32 = static_cast<double>(static_cast<float>(SINV_LINFA_TOL));
+  const int maxiter = static_cast<int>(std::min<int64_t>(5 * n, 300));
+  int calls = 0;
+  const CoreOutcome o = lobpcg_core<double>(ex, M, s, k, tol32, maxiter, true, 1e-14, false, calls, &apply);
+  st.iterations += o.iterations;
+  st.spmm_calls += inner;
+  if (!o.best_valid) return false;
+  bool accept = o.status == ST_CONVERGED;
+  if (!accept) {
+    accept = true;
+    for (int c = 0; c < k; ++c) accept = accept && (o.best_rnorm[c] < SINV_LOBPCG_QUALITY_THRESHOLD);
+  }
+  if (!accept) return false;
+  std::vector<std::pair<double, int>> pairs;
+  for (int c = 0; c < k; ++c) pairs.emplace_back(1.0 / o.best_lam[c] - SINV_SHIFT, c);
+  std::stable_sort(pairs.begin(), pairs.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+  std::vector<int> cols;
+  out.k = k;
+  out.vals.clear();
+  for (const auto& pr : pairs) {
+    out.vals.push_back(pr.first);
+    cols.push_back(pr.second);
+  }
+  out.vecs.alloc(static_cast<size_t>(n) * k, ex.stream);
+  gather_columns_dev<double, double>(ex, s.Xbest.get(), ld, out.vecs.get(), k, n, cols);
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // Randomized SVD on M = 2I - L.
 namespace {
@@ -579,8 +667,18 @@ void solve_eigenproblem_dev(const Exec& ex, const OpDev& op_in, int n_components
       }
     }
   }
-  // Level 2 (shift-invert LOBPCG with a sparse Cholesky factor) has no device
-  // implementation; the chain continues with Level 3.
+  if (want(2)) {
+    EigenResult r;
+    if (sinv_solve_dev(ex, op, n_components, seed, sqrt_deg, cfg, r, st)) {
+      const double q = max_eigenpair_residual_dev(ex, op, r);
+      if (q < SINV_LOBPCG_QUALITY_THRESHOLD || fl == 2) {
+        st.level = 2;
+        st.max_residual = q;
+        out = std::move(r);
+        return;
+      }
+    }
+  }
   if (want(3)) {
     EigenResult r;
     if (lobpcg_solve_dev(ex, op, n_components, seed, true, sqrt_deg, cfg, r, st)) {
