@@ -39,7 +39,7 @@ constexpr double SINV_SHIFT = 1e-4;                 // M = L + eps I
 constexpr double SINV_LINFA_TOL = 1e-8;
 constexpr double SINV_LOBPCG_QUALITY_THRESHOLD = 1e-6;
 constexpr double SINV_CG_RTOL = 1e-12;              // inner solve, relative residual
-constexpr int SINV_CG_MAXIT = 5000;
+constexpr int SINV_CG_MAXIT = 2000;
 constexpr int64_t DENSE_MAX_N = 8192;  // largest n the device dense EVD accepts
 
 namespace {

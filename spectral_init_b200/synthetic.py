@@ -162,6 +162,38 @@ def fuzzy_knn_graph_gpu(n: int, k: int = 15, n_clusters: int = 100, dims: int = 
     return fuzzy_graph_gpu(idx, dist, sigma, rho)
 
 
+def multi_component_graph_gpu(n_comp: int = 500, size_min: int = 20, size_max: int = 100_000, dims: int = 20,
+                              k: int = 15, seed: int = 42, device="cuda"):
+    """Block-diagonal union of independent fuzzy-kNN graphs (the batched
+    multi-component workload): component sizes log-uniform in [size_min,
+    size_max], each a seeded Gaussian mixture of 1-10 overlapping clusters in
+    `dims` dimensions, shifted to its own region of the data space.  Returns
+    (indptr int64, indices int32, data f32, n, points f32 [n, dims], sizes)."""
+    torch = _torch()
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(math.log(size_min), math.log(size_max), n_comp)).astype(np.int64)
+    ips, ixs, dvs, xs = [], [], [], []
+    node_off = 0
+    nnz_off = 0
+    for c, sz in enumerate(sizes):
+        sz = int(sz)
+        kk = min(k, sz - 1)
+        clusters = int(rng.integers(1, 11))
+        x = gaussian_mixture_gpu(sz, clusters, dims, seed * 100_003 + c, center_std=1.0, device=device)
+        x = x + torch.from_numpy(rng.normal(0.0, 100.0, dims).astype(np.float32)).to(x.device)
+        idx, dist = knn_gpu(x, kk)
+        sigma, rho = smooth_knn_gpu(dist, kk)
+        ip, ix, dv = fuzzy_graph_gpu(idx, dist, sigma, rho, prune=False)
+        ips.append(ip[:-1] + nnz_off)
+        ixs.append(ix + node_off)
+        dvs.append(dv)
+        xs.append(x)
+        node_off += sz
+        nnz_off += int(ix.numel())
+    indptr = torch.cat(ips + [torch.tensor([nnz_off], dtype=torch.int64, device=device)])
+    return indptr, torch.cat(ixs).contiguous(), torch.cat(dvs).contiguous(), node_off, torch.cat(xs), sizes
+
+
 def to_scipy(indptr, indices, data, n):
     import scipy.sparse as sp
     return sp.csr_matrix((data.cpu().numpy(), indices.cpu().numpy(), indptr.cpu().numpy()), shape=(n, n))

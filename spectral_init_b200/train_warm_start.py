@@ -90,7 +90,7 @@ def main(argv=None):
     a = p.parse_args(argv)
 
     import torch
-    from .api import get_context
+    from .api import SpectralError, get_context
     from .warm_start import WEIGHTS_PATH, DeviceLaplacian, WarmStartModel
 
     dev = torch.device("cuda", 0)
@@ -107,7 +107,11 @@ def main(argv=None):
             skipped += 1
             continue
         lap = DeviceLaplacian((g[0], g[1], g[2], n), ctx=ctx)
-        vecs, rep, level, _ = solve(ctx, lap, 0, 0)
+        try:
+            vecs, rep, level, _ = solve(ctx, lap, 0, 0)
+        except SpectralError:
+            skipped += 1
+            continue
         if level != 1 or not rep.max_residual < 1e-5:
             skipped += 1
             continue
@@ -144,11 +148,14 @@ def main(argv=None):
             continue
         lap = DeviceLaplacian((g[0], g[1], g[2], n), ctx=ctx)
         row = dict(meta)
-        for name, ws, lf in (("random", 0, 0), ("learned", 1, 0), ("learned_filtered", 1, 1)):
-            solve(ctx, lap, 1, ws, learned_filter=lf)
-            _, rep, level, sec = solve(ctx, lap, 1, ws, learned_filter=lf)
-            row[name] = {"iterations": rep.iterations, "s": round(sec, 4), "level": level,
-                         "residual": rep.max_residual}
+        try:
+            for name, ws, lf in (("random", 0, 0), ("learned", 1, 0), ("learned_filtered", 1, 1)):
+                solve(ctx, lap, 1, ws, learned_filter=lf)
+                _, rep, level, sec = solve(ctx, lap, 1, ws, learned_filter=lf)
+                row[name] = {"iterations": rep.iterations, "s": round(sec, 4), "level": level,
+                             "residual": rep.max_residual}
+        except SpectralError as e:
+            row["error"] = str(e)
         print(json.dumps({"phase": "holdout", **row}), flush=True)
     if a.eval_1m:
         from . import synthetic
