@@ -149,7 +149,13 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-constexpr int G4_TR = 64;
+constexpr int G4_TR = 128;    // rows per pipeline stage
+constexpr int G4_STAGES = 3;  // cp.async stages in flight
+
+template <class XT>
+constexpr size_t gram4_smem_bytes() {
+  return static_cast<size_t>(G4_STAGES) * G4_TR * 24 * sizeof(XT);
+}
 
 template <class XT>
 __global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const XT* __restrict__ R,
@@ -158,8 +164,11 @@ __global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const X
                                                double* partial, double* out, unsigned* counter,
                                                const int* __restrict__ stop) {
   if (stop != nullptr && *stop != 0) return;
-  __shared__ __align__(16) XT tile[2][G4_TR][24];
-  __shared__ double red[8][288];
+  // stages of [G4_TR][24] rows; after the main loop the same memory holds the
+  // per-warp reduction buffer red[8][288] (f64)
+  extern __shared__ __align__(16) unsigned char gram4_raw[];
+  XT (*tile)[G4_TR][24] = reinterpret_cast<XT (*)[G4_TR][24]>(gram4_raw);
+  double (*red)[288] = reinterpret_cast<double (*)[288]>(gram4_raw);
   __shared__ bool last;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ai = 3 * (lane >> 3);  // S column base
@@ -175,30 +184,29 @@ __global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const X
   constexpr int NCH = G4_TR * 6 * CPB;
   const int64_t ntiles = (n + G4_TR - 1) / G4_TR;
   auto load_tile = [&](int64_t t, int buf) {
-    const int64_t row0 = t * G4_TR;
-    for (int c = tid; c < NCH; c += 256) {
-      const int b = c / (G4_TR * CPB);
-      const int rem = c % (G4_TR * CPB);
-      const int r = rem / CPB, h = rem % CPB;
-      const int64_t row = row0 + r;
-      const bool ok = row < n;
-      cp_async16(&tile[buf][r][b * 4 + h * EPC], src[b] + (ok ? row : 0) * 4 + h * EPC, ok ? 16 : 0);
+    if (t < ntiles) {
+      const int64_t row0 = t * G4_TR;
+      for (int c = tid; c < NCH; c += 256) {
+        const int b = c / (G4_TR * CPB);
+        const int rem = c % (G4_TR * CPB);
+        const int r = rem / CPB, h = rem % CPB;
+        const int64_t row = row0 + r;
+        const bool ok = row < n;
+        cp_async16(&tile[buf][r][b * 4 + h * EPC], src[b] + (ok ? row : 0) * 4 + h * EPC, ok ? 16 : 0);
+      }
     }
-    cp_async_commit();
+    cp_async_commit();  // empty groups keep the group count uniform
   };
+  const int64_t step = gridDim.x;
   int64_t t = blockIdx.x;
+#pragma unroll
+  for (int s0 = 0; s0 < G4_STAGES - 1; ++s0) load_tile(t + s0 * step, s0);
   int buf = 0;
-  if (t < ntiles) load_tile(t, 0);
-  for (; t < ntiles; t += gridDim.x) {
-    const int64_t tn = t + gridDim.x;
-    if (tn < ntiles) {
-      load_tile(tn, buf ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+  for (; t < ntiles; t += step) {
+    load_tile(t + (G4_STAGES - 1) * step, (buf + G4_STAGES - 1) % G4_STAGES);
+    cp_async_wait<G4_STAGES - 1>();
     __syncthreads();
-#pragma unroll 2
+#pragma unroll 4
     for (int r = warp; r < G4_TR; r += 8) {
       const XT* row = tile[buf][r];
       const double s0 = static_cast<double>(row[ai]), s1 = static_cast<double>(row[ai + 1]),
@@ -216,8 +224,10 @@ __global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const X
       acc[2][2] = fma(s2, t2, acc[2][2]);
     }
     __syncthreads();
-    buf ^= 1;
+    buf = (buf + 1) % G4_STAGES;
   }
+  cp_async_wait<0>();
+  __syncthreads();
 #pragma unroll
   for (int p = 0; p < 3; ++p)
 #pragma unroll
@@ -867,11 +877,23 @@ void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, 
   SI_REQUIRE(nblk >= 1 && nblk <= 8 && m >= 1 && nblk * m <= GMAXW, SI_INVALID_ARGUMENT, "gram: too many columns");
   if (mode == GRAM_SYM2 && ns == 3 && nblk == 6 && m == 4 && ld == 4) {
     // the per-iteration LOBPCG Gram of 4-column blocks
+    // resident CTAs per SM from the stage memory (set once per device)
+    static int resident[2][64] = {};
+    const int ti = sizeof(XT) == 8 ? 1 : 0;
+    SI_REQUIRE(ex.device >= 0 && ex.device < 64, SI_INVALID_ARGUMENT, "gram: device ordinal");
+    if (resident[ti][ex.device] == 0) {
+      SI_CUDA(cudaFuncSetAttribute(k_gram4<XT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(gram4_smem_bytes<XT>())));
+      int r = 0;
+      SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gram4<XT>, 256, gram4_smem_bytes<XT>()));
+      resident[ti][ex.device] = std::max(1, r);
+    }
     const int64_t ntiles = (n + G4_TR - 1) / G4_TR;
-    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ex.sms) * 2)));
+    const int grid = static_cast<int>(
+        std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ex.sms) * resident[ti][ex.device])));
     w.ensure(static_cast<size_t>(grid) * 288, ex.stream);
-    k_gram4<XT><<<grid, 256, 0, ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4], blk[5], n, w.partial.get(), out,
-                                            w.counter.get(), stop);
+    k_gram4<XT><<<grid, 256, gram4_smem_bytes<XT>(), ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4], blk[5], n,
+                                                                  w.partial.get(), out, w.counter.get(), stop);
     SI_LAUNCH_CHECK();
     return;
   }
