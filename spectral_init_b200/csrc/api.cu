@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -12,9 +13,11 @@
 #include "pipeline.h"
 
 std::atomic<uint64_t> si::g_kernel_launches{0};
+thread_local uint64_t si::tl_kernel_launches = 0;
 
 struct si_model {
   int device = 0;
+  std::mutex mu;  // one forward pass at a time (components may be solved concurrently)
   si::MpnnModel m;
   si::MpnnActs acts;
   si::GemmWorkspace ws;
@@ -89,6 +92,7 @@ si::OpDev op_of(const si_operator* op) {
 bool learned_block(si_model* model, const si::Exec& ex, const si::OpDev& op, const double* sqrt_deg, int k,
                    uint64_t seed, double* x, int ld) {
   if (op.v32 == nullptr || sqrt_deg == nullptr || k > si::kMpnnOut) return false;
+  std::lock_guard<std::mutex> lock(model->mu);
   si::mpnn_features(ex, op, sqrt_deg, seed, nullptr, model->acts);
   si::mpnn_forward(ex, model->m, op, model->acts, model->ws);
   std::vector<int> cols(k);

@@ -878,7 +878,7 @@ void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, 
   if (mode == GRAM_SYM2 && ns == 3 && nblk == 6 && m == 4 && ld == 4) {
     // the per-iteration LOBPCG Gram of 4-column blocks
     // resident CTAs per SM from the stage memory (set once per device)
-    static int resident[2][64] = {};
+    static std::atomic<int> resident[2][64];
     const int ti = sizeof(XT) == 8 ? 1 : 0;
     SI_REQUIRE(ex.device >= 0 && ex.device < 64, SI_INVALID_ARGUMENT, "gram: device ordinal");
     if (resident[ti][ex.device] == 0) {
@@ -889,8 +889,9 @@ void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, 
       resident[ti][ex.device] = std::max(1, r);
     }
     const int64_t ntiles = (n + G4_TR - 1) / G4_TR;
-    const int grid = static_cast<int>(
-        std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ex.sms) * resident[ti][ex.device])));
+    // at most two CTAs per SM: the finishing CTA adds 288 partials per CTA
+    const int grid = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>(ntiles, int64_t(ex.sms) * std::min(2, resident[ti][ex.device].load()))));
     w.ensure(static_cast<size_t>(grid) * 288, ex.stream);
     k_gram4<XT><<<grid, 256, gram4_smem_bytes<XT>(), ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4], blk[5], n,
                                                                   w.partial.get(), out, w.counter.get(), stop);

@@ -19,6 +19,7 @@ namespace si {
 namespace {
 
 constexpr int DT = 1024;
+constexpr int64_t kTriMultiMin = 192;  // from this n the tridiagonalisation runs as multi-CTA steps
 
 __global__ void k_densify(int64_t n, const uint64_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
                           const double* __restrict__ vals, double diag, double* __restrict__ A) {
@@ -117,6 +118,115 @@ __global__ void __launch_bounds__(DT) k_tridiag(double* A, int n, double* d, dou
     }
     d[n - 1] = A[static_cast<int64_t>(n - 1) * n + n - 1];
   }
+}
+
+// ---- multi-CTA tridiagonalisation: the same Householder steps as k_tridiag,
+// each step three launches so the trailing-matrix passes use the whole GPU.
+// Step j:  (1) one CTA forms the reflector of column j (d, e, tau; v in vbuf
+// and in row j of A); (2) w = tau A v over the trailing rows, one warp per
+// row, per-CTA partial dots w.v, the last CTA subtracts K v with
+// K = tau (w.v) / 2 (deterministic order); (3) A -= v w^T + w v^T.
+__global__ void __launch_bounds__(256) k_tri_house(double* A, int n, int j, double* d, double* e, double* tau,
+                                                   double* vbuf) {
+  __shared__ double red[32];
+  __shared__ double s_tau, s_scal;
+  const int tid = threadIdx.x;
+  double part = 0.0;
+  for (int i = j + 2 + tid; i < n; i += blockDim.x) {
+    const double x = A[static_cast<int64_t>(i) * n + j];
+    part += x * x;
+  }
+  const double sigma = block_sum_all(part, red);
+  if (tid == 0) {
+    const double alpha = A[static_cast<int64_t>(j + 1) * n + j];
+    double t = 0.0, beta = alpha, scal = 0.0;
+    if (sigma > 0.0) {
+      const double nrm = sqrt(alpha * alpha + sigma);
+      beta = alpha >= 0.0 ? -nrm : nrm;
+      t = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    s_tau = t;
+    s_scal = scal;
+    e[j] = beta;
+    tau[j] = t;
+    d[j] = A[static_cast<int64_t>(j) * n + j];
+  }
+  __syncthreads();
+  if (s_tau == 0.0) return;
+  const double scal = s_scal;
+  for (int i = j + 1 + tid; i < n; i += blockDim.x) {
+    const double vi = (i == j + 1) ? 1.0 : A[static_cast<int64_t>(i) * n + j] * scal;
+    vbuf[i] = vi;
+    if (i >= j + 2) A[static_cast<int64_t>(j) * n + i] = vi;  // keep the reflector in row j
+  }
+}
+
+__global__ void __launch_bounds__(256) k_tri_matvec(const double* __restrict__ A, int n, int j,
+                                                    const double* __restrict__ tau, const double* __restrict__ vbuf,
+                                                    double* __restrict__ wbuf, double* __restrict__ partial,
+                                                    unsigned* __restrict__ counter) {
+  __shared__ double red[8];
+  __shared__ bool last;
+  const double t = tau[j];
+  if (t == 0.0) return;  // uniform for the grid
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r = j + 1 + blockIdx.x * 8 + warp;
+  double wv = 0.0;
+  if (r < n) {
+    double acc = 0.0;
+    const double* row = A + static_cast<int64_t>(r) * n;
+    for (int c = j + 1 + lane; c < n; c += 32) acc = fma(row[c], vbuf[c], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      wbuf[r] = t * acc;
+      wv = t * acc * vbuf[r];
+    }
+  }
+  if (lane == 0) red[warp] = wv;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += red[w];
+    partial[blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __shared__ double s_k;
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int b = 0; b < static_cast<int>(gridDim.x); ++b) s += __ldcg(&partial[b]);
+    s_k = 0.5 * t * s;
+    *counter = 0u;
+  }
+  __syncthreads();
+  const double K = s_k;
+  for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) wbuf[i] = __ldcg(&wbuf[i]) - K * vbuf[i];
+}
+
+__global__ void __launch_bounds__(256) k_tri_update(double* __restrict__ A, int n, int j,
+                                                    const double* __restrict__ tau, const double* __restrict__ vbuf,
+                                                    const double* __restrict__ wbuf) {
+  if (tau[j] == 0.0) return;
+  for (int r = j + 1 + blockIdx.x; r < n; r += gridDim.x) {
+    const double vr = vbuf[r], wr = wbuf[r];
+    double* row = A + static_cast<int64_t>(r) * n;
+    for (int c = j + 1 + threadIdx.x; c < n; c += blockDim.x) row[c] -= vr * wbuf[c] + wr * vbuf[c];
+  }
+}
+
+__global__ void k_tri_last(const double* A, int n, double* d, double* e, double* tau) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (n >= 2) {
+    d[n - 2] = A[static_cast<int64_t>(n - 2) * n + n - 2];
+    e[n - 2] = A[static_cast<int64_t>(n - 1) * n + n - 2];
+    tau[n - 2] = 0.0;
+  }
+  d[n - 1] = A[static_cast<int64_t>(n - 1) * n + n - 1];
 }
 
 // number of eigenvalues of T[l..r] smaller than x (Sturm sequence)
@@ -352,14 +462,35 @@ void dense_evd_dev(const Exec& ex, const OpDev& op, int k, double* evals_host, d
   k_mirror_lower<<<static_cast<int>(std::min<int64_t>((n * n + 255) / 256, int64_t(ex.sms) * 16)), 256, 0,
                    ex.stream>>>(n, A.get());
   SI_LAUNCH_CHECK();
-  const size_t smem = sizeof(double) * 2 * n;
-  static bool attr_set[128] = {};
-  if (ex.device >= 0 && ex.device < 128 && !attr_set[ex.device]) {
-    SI_CUDA(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 8192 * 8));
-    attr_set[ex.device] = true;
+  if (n < kTriMultiMin) {
+    // small matrices: one CTA (launch latency would dominate the step kernels)
+    const size_t smem = sizeof(double) * 2 * n;
+    static std::atomic<bool> attr_set[128];
+    if (ex.device >= 0 && ex.device < 128 && !attr_set[ex.device]) {
+      SI_CUDA(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 8192 * 8));
+      attr_set[ex.device] = true;
+    }
+    k_tridiag<<<1, DT, smem, ex.stream>>>(A.get(), static_cast<int>(n), d.get(), e.get(), tau.get());
+    SI_LAUNCH_CHECK();
+  } else {
+    const int ni = static_cast<int>(n);
+    DevBuf<double> vbuf(n, ex.stream), wbuf(n, ex.stream), partial((n + 7) / 8, ex.stream);
+    DevBuf<unsigned> counter(1, ex.stream);
+    counter.zero();
+    for (int j = 0; j + 2 < ni; ++j) {
+      const int len = ni - j - 1;
+      k_tri_house<<<1, 256, 0, ex.stream>>>(A.get(), ni, j, d.get(), e.get(), tau.get(), vbuf.get());
+      SI_LAUNCH_CHECK();
+      k_tri_matvec<<<(len + 7) / 8, 256, 0, ex.stream>>>(A.get(), ni, j, tau.get(), vbuf.get(), wbuf.get(),
+                                                         partial.get(), counter.get());
+      SI_LAUNCH_CHECK();
+      k_tri_update<<<std::min(len, ex.sms * 8), 256, 0, ex.stream>>>(A.get(), ni, j, tau.get(), vbuf.get(),
+                                                                    wbuf.get());
+      SI_LAUNCH_CHECK();
+    }
+    k_tri_last<<<1, 32, 0, ex.stream>>>(A.get(), ni, d.get(), e.get(), tau.get());
+    SI_LAUNCH_CHECK();
   }
-  k_tridiag<<<1, DT, smem, ex.stream>>>(A.get(), static_cast<int>(n), d.get(), e.get(), tau.get());
-  SI_LAUNCH_CHECK();
   DevBuf<int> bstart(n + 1, ex.stream), cand_blk(static_cast<size_t>(n) * k, ex.stream), piv(n, ex.stream),
       sel_blk(MAXM, ex.stream);
   DevBuf<double> es(n, ex.stream), cand(static_cast<size_t>(n) * k, ex.stream), lu(5 * n, ex.stream),

@@ -9,6 +9,10 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
+#include <mutex>
+#include <thread>
 #include <cfloat>
 #include <cmath>
 #include <numeric>
@@ -18,6 +22,8 @@
 
 namespace si {
 namespace {
+
+constexpr int kComponentWorkers = 16;  // host threads (one stream each) solving components
 
 __global__ void k_iota_u32p(int64_t n, uint32_t* out) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -325,26 +331,38 @@ void embed_disconnected_dev(const Exec& ex, const GraphDev& g, const uint32_t* l
     }
   }
   // ---- per component (src/multi_component.rs:261-312) -----------------------------
+  // Components are independent: worker threads, each with its own stream,
+  // take them largest first, so small components (single-CTA dense solves,
+  // latency-bound LOBPCG steps) run side by side on the GPU.  Every worker
+  // writes only its components' rows of `result`.
   result.alloc(static_cast<size_t>(n) * dims, ex.stream);
-  DevBuf<double> dmeta(dims, ex.stream);
-  GramWork gw;
-  for (int64_t c = 0; c < ncomp; ++c) {
+  SI_CUDA(cudaStreamSynchronize(ex.stream));
+  std::vector<int64_t> order(ncomp);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+    return (h_off[a + 1] - h_off[a]) > (h_off[b + 1] - h_off[b]);
+  });
+  std::atomic<int64_t> next{0};
+  std::atomic<bool> failed{false};
+  std::mutex mu;
+  std::exception_ptr first_error;
+  auto solve_one = [&](const Exec& wex, GramWork& gw, DevBuf<double>& dmeta, int64_t c) {
     const int64_t off = static_cast<int64_t>(h_off[c]);
     const int64_t sz = static_cast<int64_t>(h_off[c + 1] - h_off[c]);
     SI_CUDA(cudaMemcpyAsync(dmeta.get(), meta.data() + c * dims, sizeof(double) * dims, cudaMemcpyHostToDevice,
-                            ex.stream));
+                            wex.stream));
     if (sz < 2 * dims) {
-      k_place<<<grid_for(ex, sz * dims), 256, 0, ex.stream>>>(sz, off, perm.get(), nullptr, dims, 0.0, dmeta.get(),
-                                                               result.get());
+      k_place<<<grid_for(wex, sz * dims), 256, 0, wex.stream>>>(sz, off, perm.get(), nullptr, dims, 0.0, dmeta.get(),
+                                                                 result.get());
       SI_LAUNCH_CHECK();
-      SI_CUDA(cudaStreamSynchronize(ex.stream));
-      continue;
+      SI_CUDA(cudaStreamSynchronize(wex.stream));
+      return;
     }
     // component view: its rows are contiguous in the permuted CSR; every array
     // handed to the solver is component-relative (indptr rebased to 0)
     const uint64_t ebase = h_pptr[off];
-    DevBuf<uint64_t> sub_ptr(sz + 1, ex.stream);
-    k_rebase<<<grid_for(ex, sz + 1), 256, 0, ex.stream>>>(sz, pptr.get() + off, ebase, sub_ptr.get());
+    DevBuf<uint64_t> sub_ptr(sz + 1, wex.stream);
+    k_rebase<<<grid_for(wex, sz + 1), 256, 0, wex.stream>>>(sz, pptr.get() + off, ebase, sub_ptr.get());
     SI_LAUNCH_CHECK();
     GraphDev sub;
     sub.n = sz;
@@ -355,18 +373,49 @@ void embed_disconnected_dev(const Exec& ex, const GraphDev& g, const uint32_t* l
     DevBuf<double> coords;
     SolverStats cst;
     std::vector<double> ev;
-    embed_connected(ex, sub, dims, seed, pc, coords, cst, ev);
+    embed_connected(wex, sub, dims, seed, pc, coords, cst, ev);
+    const double mx = max_abs_dev(wex, gw, coords.get(), sz, dims, dims);
+    const double s = mx > 0.0 ? ranges[c] / mx : 1.0;
+    k_place<<<grid_for(wex, sz * dims), 256, 0, wex.stream>>>(sz, off, perm.get(), coords.get(), dims, s, dmeta.get(),
+                                                               result.get());
+    SI_LAUNCH_CHECK();
+    SI_CUDA(cudaStreamSynchronize(wex.stream));
+    std::lock_guard<std::mutex> lk(mu);
     rep.stats.iterations += cst.iterations;
     rep.stats.spmm_calls += cst.spmm_calls;
     rep.stats.level = std::max(rep.stats.level, cst.level);
     rep.stats.max_residual = std::max(rep.stats.max_residual, cst.max_residual);
-    const double mx = max_abs_dev(ex, gw, coords.get(), sz, dims, dims);
-    const double s = mx > 0.0 ? ranges[c] / mx : 1.0;
-    k_place<<<grid_for(ex, sz * dims), 256, 0, ex.stream>>>(sz, off, perm.get(), coords.get(), dims, s, dmeta.get(),
-                                                             result.get());
-    SI_LAUNCH_CHECK();
-    SI_CUDA(cudaStreamSynchronize(ex.stream));
-  }
+  };
+  auto worker = [&]() {
+    cudaStream_t st = nullptr;
+    try {
+      SI_CUDA(cudaSetDevice(ex.device));
+      SI_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      Exec wex = ex;
+      wex.stream = st;
+      GramWork gw;
+      DevBuf<double> dmeta(dims, st);
+      for (;;) {
+        const int64_t i = next.fetch_add(1);
+        if (i >= ncomp || failed.load()) break;
+        solve_one(wex, gw, dmeta, order[i]);
+      }
+    } catch (...) {
+      std::lock_guard<std::mutex> lk(mu);
+      if (!first_error) first_error = std::current_exception();
+      failed.store(true);
+    }
+    if (st != nullptr) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  };
+  const int n_workers = static_cast<int>(std::min<int64_t>(kComponentWorkers, ncomp));
+  std::vector<std::thread> pool;
+  for (int w = 1; w < n_workers; ++w) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+  if (first_error) std::rethrow_exception(first_error);
 }
 
 }  // namespace si

@@ -35,10 +35,13 @@ struct Error : std::runtime_error {
 
 // Kernels launched by this library in this process (diagnostics export).
 extern std::atomic<uint64_t> g_kernel_launches;
+// launches made by the calling host thread (graph-capture accounting)
+extern thread_local uint64_t tl_kernel_launches;
 
 #define SI_LAUNCH_CHECK()                                            \
   do {                                                               \
     ::si::g_kernel_launches.fetch_add(1, std::memory_order_relaxed); \
+    ++::si::tl_kernel_launches;                                      \
     SI_CUDA(cudaGetLastError());                                     \
   } while (0)
 

@@ -38,38 +38,8 @@ __device__ void cta_identity(double* V, int s, int ld) {
   for (int i = threadIdx.x; i < s * s; i += blockDim.x) V[(i / s) * ld + i % s] = (i / s == i % s) ? 1.0 : 0.0;
 }
 
-// Warp 0 alone: in-place lower Cholesky of a small matrix (s <= 32), the same
-// column-by-column elimination as the CTA version with warp barriers only.
-__device__ bool warp_cholesky(double* B, int s, int ld, double tol) {
-  const int lane = threadIdx.x & 31;
-  for (int j = 0; j < s; ++j) {
-    const double d = B[j * ld + j];
-    if (!(d > tol)) return false;  // every lane reads the same pivot
-    const double piv = sqrt(d);
-    __syncwarp();
-    if (lane == 0) B[j * ld + j] = piv;
-    for (int i = j + 1 + lane; i < s; i += 32) B[i * ld + j] /= piv;
-    __syncwarp();
-    const int w = s - j - 1;
-    for (int t = lane; t < w * w; t += 32) {
-      const int i = j + 1 + t / w, k = j + 1 + t % w;
-      if (k <= i) B[i * ld + k] -= B[i * ld + j] * B[k * ld + j];
-    }
-    __syncwarp();
-  }
-  return true;
-}
-
 // In-place lower Cholesky; returns false if a pivot is <= tol.
 __device__ bool cta_cholesky(double* B, int s, int ld, double tol, int* sflag) {
-  if (s <= 32) {
-    if (threadIdx.x < 32) {
-      const bool ok = warp_cholesky(B, s, ld, tol);
-      if (threadIdx.x == 0) *sflag = ok ? 0 : 1;
-    }
-    __syncthreads();
-    return *sflag == 0;
-  }
   for (int j = 0; j < s; ++j) {
     if (threadIdx.x == 0) {
       const double d = B[j * ld + j];
@@ -142,98 +112,10 @@ __device__ double cta_sum(double v, double* red) {
   return t;
 }
 
-// Rotation of the pair (a, b) of round r in the round-robin ordering; sn == 0
-// when a_ab is negligible (same skip rule in every Jacobi variant).
-__device__ __forceinline__ void jacobi_pair(const double* A, int s, int ld, int s2, int r, int p, int& a, int& b,
-                                            double& c, double& sn) {
-  if (p == 0) {
-    a = r;
-    b = s2 - 1;
-  } else {
-    a = (r + p) % (s2 - 1);
-    b = (r - p + s2 - 1) % (s2 - 1);
-  }
-  if (a > b) {
-    const int t = a;
-    a = b;
-    b = t;
-  }
-  c = 1.0;
-  sn = 0.0;
-  if (b < s) {
-    const double apq = A[a * ld + b];
-    const double app = A[a * ld + a], aqq = A[b * ld + b];
-    if (fabs(apq) > 1e-300 && fabs(apq) > DBL_EPSILON * 1e-3 * sqrt(fabs(app * aqq))) {
-      const double theta = (aqq - app) / (2.0 * apq);
-      const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-      c = 1.0 / sqrt(t * t + 1.0);
-      sn = t * c;
-    }
-  }
-}
-
-// Warp 0 alone: the parallel cyclic Jacobi of cta_jacobi for s <= 32, with
-// warp barriers between the three phases of a round instead of CTA barriers.
-__device__ void warp_jacobi(double* A, double* V, int s, int ld, double* rc, double* rs, int* ra, int* rb) {
-  const int lane = threadIdx.x & 31;
-  const int s2 = s + (s & 1);
-  const int np = s2 / 2;
-  for (int sweep = 0; sweep < 40; ++sweep) {
-    double off = 0.0, dia = 0.0;
-    for (int t = lane; t < s * s; t += 32) {
-      const int i = t / s, j = t % s;
-      const double a = A[i * ld + j];
-      if (i == j) dia += a * a; else off += a * a;
-    }
-    off = warp_sum(off);
-    dia = warp_sum(dia);
-    if (!(off > DBL_EPSILON * DBL_EPSILON * dia)) return;
-    for (int r = 0; r < s2 - 1; ++r) {
-      for (int p = lane; p < np; p += 32) {
-        int a, b;
-        double c, sn;
-        jacobi_pair(A, s, ld, s2, r, p, a, b, c, sn);
-        rc[p] = c;
-        rs[p] = sn;
-        ra[p] = a;
-        rb[p] = (b < s && sn != 0.0) ? b : -1;
-      }
-      __syncwarp();
-      for (int t = lane; t < np * s; t += 32) {  // rows a, b
-        const int p = t / s, k = t - (t / s) * s;
-        const int a = ra[p], b = rb[p];
-        if (b < 0) continue;
-        const double x = A[a * ld + k], y = A[b * ld + k];
-        A[a * ld + k] = rc[p] * x - rs[p] * y;
-        A[b * ld + k] = rs[p] * x + rc[p] * y;
-      }
-      __syncwarp();
-      for (int t = lane; t < np * s; t += 32) {  // columns a, b (the annihilated pair set to exact zero)
-        const int p = t / s, k = t - (t / s) * s;
-        const int a = ra[p], b = rb[p];
-        if (b < 0) continue;
-        const double x = A[k * ld + a], y = A[k * ld + b];
-        A[k * ld + a] = (k == b) ? 0.0 : rc[p] * x - rs[p] * y;
-        A[k * ld + b] = (k == a) ? 0.0 : rs[p] * x + rc[p] * y;
-        const double vx = V[k * ld + a], vy = V[k * ld + b];
-        V[k * ld + a] = rc[p] * vx - rs[p] * vy;
-        V[k * ld + b] = rs[p] * vx + rc[p] * vy;
-      }
-      __syncwarp();
-    }
-  }
-}
-
 // Parallel cyclic Jacobi (round-robin pairing): A <- diag, V <- eigenvectors
 // (columns).  A is symmetric s x s; V must hold the identity on entry.
 __device__ void cta_jacobi(double* A, double* V, int s, int ld, double* red, double* rc, double* rs, int* ra,
                            int* rb) {
-  if (s <= 32) {
-    __syncthreads();
-    if (threadIdx.x < 32) warp_jacobi(A, V, s, ld, rc, rs, ra, rb);
-    __syncthreads();
-    return;
-  }
   const int s2 = s + (s & 1);
   const int np = s2 / 2;
   // this thread's (pair, index) items of a round, resolved once per call
@@ -729,7 +611,7 @@ __global__ void __launch_bounds__(ST) k_small_dense(const double* __restrict__ a
 void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode, int m) {
   const int LDS = 3 * MAXM;
   const size_t smem = sizeof(double) * 4 * LDS * LDS;
-  static bool attr_set[128] = {};
+  static std::atomic<bool> attr_set[128];
   if (ex.device >= 0 && ex.device < 128 && !attr_set[ex.device]) {
     SI_CUDA(cudaFuncSetAttribute(k_small_step, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     attr_set[ex.device] = true;
@@ -742,7 +624,7 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
 void small_dense_dev(const Exec& ex, const double* a, int s, int mode, double* evals, double* evecs) {
   SI_REQUIRE(s >= 1 && s <= SMAX, SI_INVALID_ARGUMENT, "small_dense: size out of range");
   const size_t smem = sizeof(double) * 2 * SMAX * SMAX;
-  static bool attr_set[128] = {};
+  static std::atomic<bool> attr_set[128];
   if (ex.device >= 0 && ex.device < 128 && !attr_set[ex.device]) {
     SI_CUDA(cudaFuncSetAttribute(k_small_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     attr_set[ex.device] = true;

@@ -170,7 +170,7 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
   }
   constexpr int kGraphBatch = 8;
   cudaGraphExec_t exec = nullptr;
-  const uint64_t launches_before_capture = g_kernel_launches.load();
+  const uint64_t launches_before_capture = tl_kernel_launches;
   {
     cudaGraph_t graph = nullptr;
     SI_CUDA(cudaStreamBeginCapture(ex.stream, cudaStreamCaptureModeThreadLocal));
@@ -187,8 +187,9 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
     SI_CUDA(ie);
   }
   // captured launches are not executions; each graph replay adds its kernels below
-  const uint64_t per_replay = g_kernel_launches.load() - launches_before_capture;
-  g_kernel_launches.store(launches_before_capture);
+  const uint64_t per_replay = tl_kernel_launches - launches_before_capture;
+  tl_kernel_launches = launches_before_capture;
+  g_kernel_launches.fetch_sub(per_replay);
   struct ExecGuard {
     cudaGraphExec_t e;
     ~ExecGuard() {
@@ -204,6 +205,7 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
     SI_REQUIRE(launched <= maxiter + 2 * kGraphBatch, SI_CUDA_ERROR, "lobpcg: device loop did not terminate");
     SI_CUDA(cudaGraphLaunch(exec, ex.stream));
     g_kernel_launches.fetch_add(per_replay);
+    tl_kernel_launches += per_replay;
     launched += kGraphBatch;
   }
   return finish_core(ex, s, spmm_calls);

@@ -454,7 +454,7 @@ template <class VT, class XT, int LD, int G>
 void launch_tiled(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                   const int* stop) {
   const int smem = static_cast<int>(sizeof(TileSmem<VT>));
-  static int resident[128] = {};  // per device: resident CTAs per SM (0 = not set up)
+  static std::atomic<int> resident[128];  // per device: resident CTAs per SM (0 = not set up)
   const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
   if (resident[dev] == 0) {
     SI_CUDA(cudaFuncSetAttribute(k_spmm_tiled<VT, XT, LD, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
