@@ -151,21 +151,25 @@ __device__ __forceinline__ void cp_async_wait() {
 
 constexpr int G4_TR = 128;    // rows per pipeline stage
 constexpr int G4_STAGES = 3;  // cp.async stages in flight
+constexpr int G4_THREADS = 512;
+constexpr int G4_WARPS = G4_THREADS / 32;
 
 template <class XT>
 constexpr size_t gram4_smem_bytes() {
   return static_cast<size_t>(G4_STAGES) * G4_TR * 24 * sizeof(XT);
 }
+static_assert(gram4_smem_bytes<float>() >= sizeof(double) * G4_WARPS * 288,
+              "the stage memory must hold the per-warp reduction buffer");
 
 template <class XT>
-__global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const XT* __restrict__ R,
+__global__ void __launch_bounds__(G4_THREADS) k_gram4(const XT* __restrict__ X, const XT* __restrict__ R,
                                                const XT* __restrict__ P, const XT* __restrict__ AX,
                                                const XT* __restrict__ AR, const XT* __restrict__ AP, int64_t n,
                                                double* partial, double* out, unsigned* counter,
                                                const int* __restrict__ stop) {
   if (stop != nullptr && *stop != 0) return;
   // stages of [G4_TR][24] rows; after the main loop the same memory holds the
-  // per-warp reduction buffer red[8][288] (f64)
+  // per-warp reduction buffer red[G4_WARPS][288] (f64)
   extern __shared__ __align__(16) unsigned char gram4_raw[];
   XT (*tile)[G4_TR][24] = reinterpret_cast<XT (*)[G4_TR][24]>(gram4_raw);
   double (*red)[288] = reinterpret_cast<double (*)[288]>(gram4_raw);
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const X
   auto load_tile = [&](int64_t t, int buf) {
     if (t < ntiles) {
       const int64_t row0 = t * G4_TR;
-      for (int c = tid; c < NCH; c += 256) {
+      for (int c = tid; c < NCH; c += G4_THREADS) {
         const int b = c / (G4_TR * CPB);
         const int rem = c % (G4_TR * CPB);
         const int r = rem / CPB, h = rem % CPB;
@@ -207,7 +211,7 @@ __global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const X
     cp_async_wait<G4_STAGES - 1>();
     __syncthreads();
 #pragma unroll 4
-    for (int r = warp; r < G4_TR; r += 8) {
+    for (int r = warp; r < G4_TR; r += G4_WARPS) {
       const XT* row = tile[buf][r];
       const double s0 = static_cast<double>(row[ai]), s1 = static_cast<double>(row[ai + 1]),
                    s2 = static_cast<double>(row[ai + 2]);
@@ -234,10 +238,10 @@ __global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const X
     for (int q = 0; q < 3; ++q) red[warp][(ai + p) * 24 + bj + q] = acc[p][q];
   __syncthreads();
   const int G = gridDim.x;
-  for (int e = tid; e < 288; e += 256) {
+  for (int e = tid; e < 288; e += G4_THREADS) {
     double s = 0.0;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) s += red[w][e];
+    for (int w = 0; w < G4_WARPS; ++w) s += red[w][e];
     partial[static_cast<int64_t>(e) * G + blockIdx.x] = s;
   }
   __threadfence();
@@ -247,7 +251,7 @@ __global__ void __launch_bounds__(256) k_gram4(const XT* __restrict__ X, const X
   if (!last) return;
   __threadfence();
   // finishing CTA: four entries per warp pass so a lane keeps many loads in flight
-  for (int e0 = warp * 4; e0 < 288; e0 += 32) {
+  for (int e0 = warp * 4; e0 < 288; e0 += 4 * G4_WARPS) {
     double s[4] = {0.0, 0.0, 0.0, 0.0};
     for (int c = lane; c < G; c += 32) {
 #pragma unroll
@@ -885,7 +889,7 @@ void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, 
       SI_CUDA(cudaFuncSetAttribute(k_gram4<XT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(gram4_smem_bytes<XT>())));
       int r = 0;
-      SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gram4<XT>, 256, gram4_smem_bytes<XT>()));
+      SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gram4<XT>, G4_THREADS, gram4_smem_bytes<XT>()));
       resident[ti][ex.device] = std::max(1, r);
     }
     const int64_t ntiles = (n + G4_TR - 1) / G4_TR;
@@ -893,7 +897,7 @@ void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, 
     const int grid = static_cast<int>(std::max<int64_t>(
         1, std::min<int64_t>(ntiles, int64_t(ex.sms) * std::min(2, resident[ti][ex.device].load()))));
     w.ensure(static_cast<size_t>(grid) * 288, ex.stream);
-    k_gram4<XT><<<grid, 256, gram4_smem_bytes<XT>(), ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4], blk[5], n,
+    k_gram4<XT><<<grid, G4_THREADS, gram4_smem_bytes<XT>(), ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4], blk[5], n,
                                                                   w.partial.get(), out, w.counter.get(), stop);
     SI_LAUNCH_CHECK();
     return;

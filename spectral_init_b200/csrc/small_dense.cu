@@ -31,6 +31,7 @@ struct SmallSmem {
   double* B;
   double* V;
   double* Z;
+  double* T;  // second buffer of A for the double-buffered Jacobi
   int ld;
 };
 
@@ -110,6 +111,112 @@ __device__ double cta_sum(double v, double* red) {
   for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) t += red[i];
   __syncthreads();
   return t;
+}
+
+// Parallel cyclic Jacobi with one update phase per round: the round's
+// disjoint rotations J are applied as A' = J^T A J and V' = V J in a single
+// pass into second buffers (every element of A' depends on a 2 x 2 block of
+// A), so a round is two barriers.  The rotation angle uses one square root,
+// one division and one reciprocal square root:
+//   t = h sgn(d) / (|d| + sqrt(d^2 + h^2)),  d = a_qq - a_pp, h = 2 a_pq,
+//   c = 1/sqrt(1 + t^2), s = t c     (the smaller root of t^2 + 2 (d/h) t - 1).
+// On return A (diagonal) and V hold the result.
+__device__ void cta_jacobi_db(double* A, double* V, double* A2, double* V2, int s, int ld, double* red) {
+  __shared__ double al[3 * MAXM + 2], be[3 * MAXM + 2];
+  __shared__ int pq[3 * MAXM + 2], rot[3 * MAXM + 2];
+  const int s2 = s + (s & 1);
+  const int np = s2 / 2;
+  double* cur = A;
+  double* nxt = A2;
+  double* vc = V;
+  double* vn = V2;
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
+      const int i = t / s, j = t - (t / s) * s;
+      const double a = cur[i * ld + j];
+      if (i == j) dia += a * a; else off += a * a;
+    }
+    off = cta_sum(off, red);
+    dia = cta_sum(dia, red);
+    if (!(off > DBL_EPSILON * DBL_EPSILON * dia)) break;
+    for (int r = 0; r < s2 - 1; ++r) {
+      for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        int a, b;
+        if (p == 0) {
+          a = r;
+          b = s2 - 1;
+        } else {
+          a = (r + p) % (s2 - 1);
+          b = (r - p + s2 - 1) % (s2 - 1);
+        }
+        if (a > b) {
+          const int t = a;
+          a = b;
+          b = t;
+        }
+        double c = 1.0, sn = 0.0;
+        bool rotate = false;
+        if (b < s) {
+          const double apq = cur[a * ld + b];
+          const double app = cur[a * ld + a], aqq = cur[b * ld + b];
+          const double tiny = DBL_EPSILON * 1e-3;
+          if (fabs(apq) > 1e-300 && apq * apq > tiny * tiny * fabs(app * aqq)) {
+            const double d = aqq - app, h = 2.0 * apq;
+            const double t = (d >= 0.0 ? h : -h) / (fabs(d) + sqrt(fma(d, d, h * h)));
+            c = rsqrt(fma(t, t, 1.0));
+            sn = t * c;
+            rotate = true;
+          }
+        }
+        // new row/column a = c a - s b ; new b = s a + c b
+        al[a] = c;
+        be[a] = -sn;
+        pq[a] = (b < s) ? b : a;
+        rot[a] = rotate;
+        if (b < s) {
+          al[b] = c;
+          be[b] = sn;
+          pq[b] = a;
+          rot[b] = rotate;
+        }
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < 2 * s * s; t += blockDim.x) {
+        if (t < s * s) {
+          const int i = t / s, j = t - (t / s) * s;
+          const int qi = pq[i], qj = pq[j];
+          double v;
+          if (rot[i] && qi == j) {
+            v = 0.0;  // the annihilated pair: exact zero
+          } else {
+            v = al[i] * (al[j] * cur[i * ld + j] + be[j] * cur[i * ld + qj]) +
+                be[i] * (al[j] * cur[qi * ld + j] + be[j] * cur[qi * ld + qj]);
+          }
+          nxt[i * ld + j] = v;
+        } else {
+          const int u = t - s * s;
+          const int k = u / s, j = u - (u / s) * s;
+          vn[k * ld + j] = al[j] * vc[k * ld + j] + be[j] * vc[k * ld + pq[j]];
+        }
+      }
+      __syncthreads();
+      double* tmp = cur;
+      cur = nxt;
+      nxt = tmp;
+      tmp = vc;
+      vc = vn;
+      vn = tmp;
+    }
+  }
+  if (cur != A) {
+    for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
+      const int i = t / s, j = t - (t / s) * s;
+      A[i * ld + j] = cur[i * ld + j];
+      V[i * ld + j] = vc[i * ld + j];
+    }
+  }
+  __syncthreads();
 }
 
 // Parallel cyclic Jacobi (round-robin pairing): A <- diag, V <- eigenvectors
@@ -334,7 +441,8 @@ __device__ bool cta_rr_general(const double* gb, const double* ga, int P, const 
   __syncthreads();
   cta_identity(sm.V, s, ld);
   __syncthreads();
-  cta_jacobi(sm.A, sm.V, s, ld, red, rc, rs, ra, rb);
+  if (s <= 3 * MAXM) cta_jacobi_db(sm.A, sm.V, sm.T, sm.Z, s, ld, red);
+  else cta_jacobi(sm.A, sm.V, s, ld, red, rc, rs, ra, rb);
   if (threadIdx.x == 0) {
     sort_eigs(sm.A, s, ld, order);
     if (largest) {
@@ -370,7 +478,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
   __shared__ int ra[SMAX / 2 + 1], rb[SMAX / 2 + 1], order[3 * MAXM], idx[3 * MAXM];
   __shared__ int sflag, sdone, s_na, s_withp;
   const int LDS = 3 * MAXM;
-  SmallSmem sm{smem, smem + LDS * LDS, smem + 2 * LDS * LDS, smem + 3 * LDS * LDS, LDS};
+  SmallSmem sm{smem, smem + LDS * LDS, smem + 2 * LDS * LDS, smem + 3 * LDS * LDS, smem + 4 * LDS * LDS, LDS};
   const int m = ctrl->m;
   const int P = ns * m;
   const double* gb = gram;
@@ -421,7 +529,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
     __syncthreads();
     cta_identity(sm.V, m, LDS);
     __syncthreads();
-    cta_jacobi(sm.A, sm.V, m, LDS, red, rc, rs, ra, rb);
+    cta_jacobi_db(sm.A, sm.V, sm.T, sm.Z, m, LDS, red);
     if (threadIdx.x == 0) {
       sort_eigs(sm.A, m, LDS, order);
       for (int q = 0; q < m; ++q) ctrl->lam[q] = sm.A[order[q] * LDS + order[q]];
@@ -610,7 +718,7 @@ __global__ void __launch_bounds__(ST) k_small_dense(const double* __restrict__ a
 
 void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode, int m) {
   const int LDS = 3 * MAXM;
-  const size_t smem = sizeof(double) * 4 * LDS * LDS;
+  const size_t smem = sizeof(double) * 5 * LDS * LDS;
   static std::atomic<bool> attr_set[128];
   if (ex.device >= 0 && ex.device < 128 && !attr_set[ex.device]) {
     SI_CUDA(cudaFuncSetAttribute(k_small_step, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));

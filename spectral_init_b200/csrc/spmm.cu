@@ -34,7 +34,9 @@ __device__ __forceinline__ T ld_stream(const T* p) {
   return __ldcs(p);
 }
 
-// Vector gather of one x row of LD elements into f64 registers.
+// Vector gather of one x row of LD elements into f64 registers.  The 4-wide
+// rows bypass L1 (.cg): the rows a warp gathers are scattered over the block,
+// so an L1 allocation is rarely reused and costs L1 fill bandwidth.
 template <class XT, int LD>
 struct RowLoad;
 
@@ -44,7 +46,7 @@ struct RowLoad<double, LD> {
 #pragma unroll
     for (int q = 0; q < LD / 4; ++q) {
       double a, b, c, d;
-      asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+      asm volatile("ld.global.cg.v4.f64 {%0,%1,%2,%3}, [%4];"
                    : "=d"(a), "=d"(b), "=d"(c), "=d"(d)
                    : "l"(p + 4 * q));
       v[4 * q + 0] = a;
@@ -58,7 +60,7 @@ struct RowLoad<double, LD> {
 template <>
 struct RowLoad<float, 4> {
   __device__ __forceinline__ static void run(const float* p, double (&v)[4]) {
-    float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    float4 t = __ldcg(reinterpret_cast<const float4*>(p));
     v[0] = t.x;
     v[1] = t.y;
     v[2] = t.z;
