@@ -40,22 +40,31 @@ struct OpDev {
   const int64_t* row_blocks = nullptr;
   const uint64_t* block_ptr = nullptr;  // indptr[row_blocks[b]]
   int64_t n_blocks = 0;
+  // finer partition (about kGatherBlockNnz entries) for the TMA-gather SpMM
+  const int64_t* gather_blocks = nullptr;
+  const uint64_t* gather_ptr = nullptr;
+  int64_t n_gather_blocks = 0;
 };
 
 constexpr int kSpmmBlockNnz = 1024;   // target entries per row block
 constexpr int kSpmmBlockCap = 2048;   // entries a block may hold in shared memory
 constexpr int kSpmmBlockRows = 1024;  // rows a block may hold in shared memory
+constexpr int kGatherBlockNnz = 384;  // target entries per TMA-gather block
+constexpr int kGatherCap = 512;       // entries a TMA-gather block may stage
 
 // Row partition of an operator for the tiled SpMM (device array of
 // n_blocks + 1 row starts, owned by the caller).
 struct RowBlocks {
-  DevBuf<int64_t> starts;
-  DevBuf<uint64_t> ptrs;
-  int64_t n_blocks = 0;
+  DevBuf<int64_t> starts, gstarts;
+  DevBuf<uint64_t> ptrs, gptrs;
+  int64_t n_blocks = 0, n_gblocks = 0;
   void attach(OpDev& op) const {
     op.row_blocks = starts.get();
     op.block_ptr = ptrs.get();
     op.n_blocks = n_blocks;
+    op.gather_blocks = gstarts.get();
+    op.gather_ptr = gptrs.get();
+    op.n_gather_blocks = n_gblocks;
   }
 };
 void make_row_blocks(const Exec& ex, const OpDev& op, RowBlocks& rb);

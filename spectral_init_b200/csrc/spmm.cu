@@ -19,12 +19,18 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <string>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "si_internal.h"
+#include "umma.cuh"
+#include "umma_gemm.h"
 
 namespace si {
 namespace {
@@ -366,15 +372,16 @@ __global__ void k_block_ptrs(int64_t nblk, const int64_t* __restrict__ rblk, con
     out[b] = indptr[rblk[b]];
 }
 
-// row_blocks[b] = first row whose start offset is >= b * kSpmmBlockNnz
-__global__ void k_row_blocks(int64_t n, const uint64_t* __restrict__ indptr, int64_t nblk, int64_t* out) {
+// row_blocks[b] = first row whose start offset is >= b * per
+__global__ void k_row_blocks(int64_t n, const uint64_t* __restrict__ indptr, int64_t nblk, int64_t per,
+                             int64_t* out) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; b <= nblk; b += stride) {
     if (b == nblk) {
       out[b] = n;
       continue;
     }
-    const uint64_t target = static_cast<uint64_t>(b) * kSpmmBlockNnz;
+    const uint64_t target = static_cast<uint64_t>(b) * static_cast<uint64_t>(per);
     int64_t lo = 0, hi = n;  // first r in [0, n] with indptr[r] >= target
     while (lo < hi) {
       const int64_t mid = lo + (hi - lo) / 2;
@@ -430,6 +437,213 @@ __global__ void __launch_bounds__(256) k_spmm_generic(int64_t n, const uint64_t*
   }
 }
 
+// TMA-gather kernel (f32 values, 4-wide f32 rows): the x rows of a block's
+// entries are fetched by tile::gather4 copies (four rows per instruction,
+// through the TMA unit instead of per-lane loads) into a double-buffered
+// shared-memory staging area, while the previous block is computed from it.
+// A block (about kGatherBlockNnz entries, at most kGatherCap) is gathered
+// into 128-byte slots of four 16-byte rows.  Waits give up after one second
+// and record an error instead of hanging; blocks that do not fit the staging
+// area use plain gathers.
+constexpr int kGatherSlots = kGatherCap / 4;
+
+template <int G>
+__device__ __forceinline__ void gather_row(int64_t row, uint64_t s, uint64_t e, uint64_t p0, const float* slots,
+                                           const float* __restrict__ vals, double diag, const float* __restrict__ x,
+                                           float* __restrict__ y, const Epilogue<float>& ep, int sub, unsigned mask,
+                                           bool writer) {
+  constexpr int LD = 4;
+  constexpr int W = GroupReduce<LD, G>::W;
+  const int obase = GroupReduce<LD, G>::base_of(sub);
+  double own[W], addz[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) {
+    own[c] = 0.0;
+    addz[c] = 0.0;
+    if (writer) {
+      const int64_t off = row * LD + obase + c;
+      own[c] = diag * static_cast<double>(x[off]);
+      if (ep.z1) addz[c] = ep.beta * static_cast<double>(ep.z1[off]);
+      if (ep.z2) addz[c] = fma(ep.gamma, static_cast<double>(ep.z2[off]), addz[c]);
+      if (ep.z3) addz[c] = fma(ep.delta, static_cast<double>(ep.z3[off]), addz[c]);
+    }
+  }
+  double acc[LD] = {0.0, 0.0, 0.0, 0.0};
+  for (uint64_t k = s + sub; k < e; k += G) {
+    const uint64_t q = k - p0;  // entry within the block: slot q / 4, row q % 4 of the slot
+    const float4 xr = *reinterpret_cast<const float4*>(slots + (q >> 2) * 32 + (q & 3) * 4);
+    const double v = static_cast<double>(__ldcs(vals + k));
+    acc[0] = fma(v, static_cast<double>(xr.x), acc[0]);
+    acc[1] = fma(v, static_cast<double>(xr.y), acc[1]);
+    acc[2] = fma(v, static_cast<double>(xr.z), acc[2]);
+    acc[3] = fma(v, static_cast<double>(xr.w), acc[3]);
+  }
+  const int base = GroupReduce<LD, G>::run(acc, sub, mask);
+  if (writer) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      const int64_t off = row * LD + base + c;
+      y[off] = static_cast<float>(fma(ep.alpha, own[c] + acc[c], addz[c]));
+    }
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_spmm_gather(const __grid_constant__ CUtensorMap xmap, int64_t n,
+                                                     const uint64_t* __restrict__ indptr,
+                                                     const uint32_t* __restrict__ indices,
+                                                     const float* __restrict__ vals, const int64_t* __restrict__ rblk,
+                                                     const uint64_t* __restrict__ bptr, int64_t nblk, double diag,
+                                                     const float* __restrict__ x, float* __restrict__ y,
+                                                     Epilogue<float> ep, const int* __restrict__ stop, int* err) {
+  if (stop != nullptr && *stop != 0) return;
+  __shared__ __align__(128) float slots[2][kGatherSlots][32];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int sub = lane & (G - 1);
+  const unsigned mask = group_mask<G>(lane);
+  const bool writer = group_writer<4, G>(sub);
+  const int group = tid / G;
+  constexpr int NG = 256 / G;
+  if (tid == 0) {
+    umma::mbar_init(&mbar[0], 1);
+    umma::mbar_init(&mbar[1], 1);
+    umma::fence_mbar_init();
+    umma::tma_prefetch_desc(&xmap);
+    s_bad = 0;
+  }
+  __syncthreads();
+  uint32_t phase[2] = {0u, 0u};
+  auto info = [&](int64_t b) {
+    BlockInfo bi;
+    if (b < nblk) {
+      bi.r0 = rblk[b];
+      bi.r1 = rblk[b + 1];
+      bi.p0 = bptr[b];
+      bi.p1 = bptr[b + 1];
+    }
+    return bi;
+  };
+  auto staged = [](const BlockInfo& bi) { return bi.p1 > bi.p0 && (bi.p1 - bi.p0) <= kGatherCap; };
+  // all threads: one thread posts the byte count, then every thread issues its gathers
+  auto issue = [&](const BlockInfo& bi, int st) {
+    const int ne = static_cast<int>(bi.p1 - bi.p0);
+    const int ng = (ne + 3) / 4;
+    if (tid == 0) umma::mbar_arrive_expect_tx(&mbar[st], static_cast<uint32_t>(ng) * 64u);
+    __syncthreads();
+    const int32_t pad = static_cast<int32_t>(__ldg(indices + bi.p0));  // a valid row for the unused tail
+    for (int g = tid; g < ng; g += 256) {
+      int32_t r[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint64_t k = bi.p0 + 4 * g + q;
+        r[q] = k < bi.p1 ? static_cast<int32_t>(__ldg(indices + k)) : pad;
+      }
+      umma::tma_gather4(&slots[st][g][0], &xmap, &mbar[st], 0, r[0], r[1], r[2], r[3]);
+    }
+  };
+  const int64_t step = gridDim.x;
+  int64_t b = blockIdx.x;
+  int st = 0;
+  bool pending[2] = {false, false};  // a stage with copies not yet waited for
+  bool tma_on = true;                // cleared (uniformly) after a wait gave up
+  BlockInfo cur = info(b);
+  bool cur_staged = b < nblk && staged(cur);
+  if (cur_staged) {
+    issue(cur, 0);
+    pending[0] = true;
+  }
+  for (; b < nblk; b += step) {
+    const BlockInfo nxt = info(b + step);
+    const bool nxt_staged = tma_on && b + step < nblk && staged(nxt);
+    if (nxt_staged) {
+      issue(nxt, st ^ 1);
+      pending[st ^ 1] = true;
+    }
+    if (cur_staged) {
+      if (umma::mbar_wait(&mbar[st], phase[st])) {
+        phase[st] ^= 1u;
+        pending[st] = false;
+      } else {
+        s_bad = 1;
+      }
+    }
+    __syncthreads();
+    if (s_bad) tma_on = false;
+    if (cur_staged && tma_on) {
+      for (int64_t rr = cur.r0 + group; rr < cur.r1; rr += NG)
+        gather_row<G>(rr, indptr[rr], indptr[rr + 1], cur.p0, &slots[st][0][0], vals, diag, x, y, ep, sub, mask,
+                      writer);
+    } else {
+      const GlobalStream<float> src{indices, vals};
+      for (int64_t rr = cur.r0 + group; rr < cur.r1; rr += NG)
+        spmm_row<float, float, 4, G>(rr, indptr[rr], indptr[rr + 1], src, diag, x, y, ep, sub, mask, writer);
+    }
+    __syncthreads();
+    st ^= 1;
+    cur = nxt;
+    cur_staged = nxt_staged;
+  }
+  if (s_bad) {
+    // a wait gave up (those blocks were computed with plain gathers): let the
+    // copies still in flight land, within the same limit, before exit
+    for (int s2 = 0; s2 < 2; ++s2)
+      if (pending[s2]) umma::mbar_wait(&mbar[s2], phase[s2]);
+    if (tid == 0) atomicExch(err, 1);
+    __syncthreads();
+  }
+}
+
+CUtensorMap x_rows_map(const float* x, int64_t n) {
+  SI_REQUIRE(reinterpret_cast<uintptr_t>(x) % 16 == 0, SI_INVALID_ARGUMENT, "spmm: x not 16-byte aligned");
+  SI_REQUIRE(n < (int64_t(1) << 31), SI_INVALID_ARGUMENT, "spmm: too many rows for the gather path");
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {4, static_cast<cuuint64_t>(n)};
+  const cuuint64_t strides[1] = {16};
+  const cuuint32_t box[2] = {4, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(x), dims,
+                                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  SI_REQUIRE(r == CUDA_SUCCESS, SI_CUDA_ERROR, "cuTensorMapEncodeTiled (x rows) failed");
+  return map;
+}
+
+// error flag of the gather kernel, one per device (set only by a timed-out wait)
+int* gather_err(const Exec& ex) {
+  static std::mutex mu;
+  static int* flags[128] = {};
+  std::lock_guard<std::mutex> lk(mu);
+  const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
+  if (flags[dev] == nullptr) {
+    SI_CUDA(cudaMalloc(reinterpret_cast<void**>(&flags[dev]), sizeof(int)));
+    SI_CUDA(cudaMemset(flags[dev], 0, sizeof(int)));
+  }
+  return flags[dev];
+}
+
+template <int G>
+void launch_gather(const Exec& ex, const OpDev& op, const float* vals, const float* x, float* y,
+                   const Epilogue<float>& ep, const int* stop) {
+  const CUtensorMap map = x_rows_map(x, op.n);
+  int per_sm = 0;
+  static std::atomic<int> resident[128];
+  const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
+  if (resident[dev] == 0) {
+    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmm_gather<G>, 256, 0));
+    resident[dev] = std::max(per_sm, 1);
+  }
+  const int grid = static_cast<int>(
+      std::max<int64_t>(1, std::min<int64_t>(op.n_gather_blocks, int64_t(ex.sms) * resident[dev])));
+  k_spmm_gather<G><<<grid, 256, 0, ex.stream>>>(map, op.n, op.indptr, op.indices, vals, op.gather_blocks,
+                                                op.gather_ptr, op.n_gather_blocks, op.diag, x, y, ep, stop,
+                                                gather_err(ex));
+  SI_LAUNCH_CHECK();
+}
+
 template <class VT, class XT, int LD, int G>
 void launch_vec(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                 const int* stop) {
@@ -481,6 +695,15 @@ void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const 
     case 16: launch_vec<VT, XT, LD, 16>(ex, op, vals, x, y, ep, stop); break;
     case 104: launch_tiled<VT, XT, LD, 4>(ex, op, vals, x, y, ep, stop); break;
     case 108: launch_tiled<VT, XT, LD, 8>(ex, op, vals, x, y, ep, stop); break;
+    case 204:
+    case 208:
+      if constexpr (std::is_same<VT, float>::value && std::is_same<XT, float>::value && LD == 4) {
+        if (g == 204) launch_gather<4>(ex, op, vals, x, y, ep, stop);
+        else launch_gather<8>(ex, op, vals, x, y, ep, stop);
+      } else {
+        launch_vec<VT, XT, LD, 8>(ex, op, vals, x, y, ep, stop);
+      }
+      break;
     default: launch_vec<VT, XT, LD, 32>(ex, op, vals, x, y, ep, stop); break;
   }
 }
@@ -503,13 +726,40 @@ struct TuneKey {
 std::mutex g_tune_mu;
 std::map<TuneKey, int> g_tune;
 
+// Kernel override for tuning and tests: SPECTRAL_INIT_SPMM_KERNEL = vec4 | vec8 |
+// vec16 | vec32 | tiled4 | tiled8 | gather4 | gather8 (unset or "auto": the
+// autotuner).  A choice the operator or the types cannot use is ignored.
+template <class VT, class XT, int LD>
+int forced_choice(const OpDev& op, bool tiled) {
+  const char* env = std::getenv("SPECTRAL_INIT_SPMM_KERNEL");
+  if (env == nullptr) return 0;
+  const std::string v(env);
+  static const std::pair<const char*, int> names[] = {{"vec4", 4},     {"vec8", 8},       {"vec16", 16},
+                                                      {"vec32", 32},   {"tiled4", 104},   {"tiled8", 108},
+                                                      {"gather4", 204}, {"gather8", 208}};
+  for (const auto& nm : names) {
+    if (v != nm.first) continue;
+    const int c = nm.second;
+    if (c > 100 && c < 200 && !tiled) return 0;
+    if (c > 200 && !(std::is_same<VT, float>::value && std::is_same<XT, float>::value && LD == 4 &&
+                     op.gather_blocks != nullptr && op.n_gather_blocks > 0))
+      return 0;
+    return c;
+  }
+  return 0;
+}
+
 template <class VT, class XT, int LD>
 void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                 const int* stop) {
   const bool tiled = op.row_blocks != nullptr && op.n_blocks > 0;
   const TuneKey key{ex.device, op.indptr, op.n, op.nnz, LD, static_cast<int>(sizeof(VT)),
                     static_cast<int>(sizeof(XT)), tiled ? 1 : 0};
-  int g = 0;
+  int g = forced_choice<VT, XT, LD>(op, tiled);
+  if (g != 0) {
+    launch_lanes<VT, XT, LD>(g, ex, op, vals, x, y, ep, stop);
+    return;
+  }
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
@@ -530,6 +780,11 @@ void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT
       if (tiled) {
         cands.push_back(104);
         cands.push_back(108);
+      }
+      if (std::is_same<VT, float>::value && std::is_same<XT, float>::value && LD == 4 &&
+          op.gather_blocks != nullptr && op.n_gather_blocks > 0) {
+        cands.push_back(204);
+        cands.push_back(208);
       }
       for (int cand : cands) {
         launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
@@ -574,14 +829,18 @@ void dispatch(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* 
 }  // namespace
 
 void make_row_blocks(const Exec& ex, const OpDev& op, RowBlocks& rb) {
-  rb.n_blocks = std::max<int64_t>(1, (op.nnz + kSpmmBlockNnz - 1) / kSpmmBlockNnz);
-  rb.starts.alloc(rb.n_blocks + 1, ex.stream);
-  const int grid = static_cast<int>(std::min<int64_t>((rb.n_blocks + 256) / 256, int64_t(ex.sms) * 8));
-  k_row_blocks<<<std::max(grid, 1), 256, 0, ex.stream>>>(op.n, op.indptr, rb.n_blocks, rb.starts.get());
-  SI_LAUNCH_CHECK();
-  rb.ptrs.alloc(rb.n_blocks + 1, ex.stream);
-  k_block_ptrs<<<std::max(grid, 1), 256, 0, ex.stream>>>(rb.n_blocks, rb.starts.get(), op.indptr, rb.ptrs.get());
-  SI_LAUNCH_CHECK();
+  auto build = [&](int64_t per, int64_t& nb, DevBuf<int64_t>& starts, DevBuf<uint64_t>& ptrs) {
+    nb = std::max<int64_t>(1, (op.nnz + per - 1) / per);
+    starts.alloc(nb + 1, ex.stream);
+    const int grid = static_cast<int>(std::min<int64_t>((nb + 256) / 256, int64_t(ex.sms) * 8));
+    k_row_blocks<<<std::max(grid, 1), 256, 0, ex.stream>>>(op.n, op.indptr, nb, per, starts.get());
+    SI_LAUNCH_CHECK();
+    ptrs.alloc(nb + 1, ex.stream);
+    k_block_ptrs<<<std::max(grid, 1), 256, 0, ex.stream>>>(nb, starts.get(), op.indptr, ptrs.get());
+    SI_LAUNCH_CHECK();
+  };
+  build(kSpmmBlockNnz, rb.n_blocks, rb.starts, rb.ptrs);
+  build(kGatherBlockNnz, rb.n_gblocks, rb.gstarts, rb.gptrs);
 }
 
 int spmm_group_lanes(const OpDev& op) {

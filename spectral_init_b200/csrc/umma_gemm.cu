@@ -225,7 +225,9 @@ __global__ void k_sum_splits(const float* __restrict__ part, int splits, int64_t
   }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+}  // namespace
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static std::once_flag once;
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   std::call_once(once, [] {
@@ -239,6 +241,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
+namespace {
+
 // 2-D bf16 tensor map over rows x cols (row pitch ld elements), box 64 x box_rows.
 CUtensorMap make_map(const __nv_bfloat16* ptr, int64_t rows, int64_t cols, int64_t ld, int box_rows) {
   SI_REQUIRE(reinterpret_cast<uintptr_t>(ptr) % 16 == 0, SI_INVALID_ARGUMENT, "gemm: operand not 16-byte aligned");
@@ -249,7 +253,7 @@ CUtensorMap make_map(const __nv_bfloat16* ptr, int64_t rows, int64_t cols, int64
   const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld * 2)};
   const cuuint32_t box[2] = {static_cast<cuuint32_t>(BK), static_cast<cuuint32_t>(box_rows)};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), dims,
+  const CUresult r = tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), dims,
                                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   SI_REQUIRE(r == CUDA_SUCCESS, SI_CUDA_ERROR, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include "si_internal.h"
 
@@ -27,6 +28,9 @@ struct GemmWorkspace {
 // k_splits > 1 splits K across CTAs (f32 modes, ldo == N) and adds the slabs in order.
 void gemm_bf16_nt(const Exec& ex, int64_t M, int N, int64_t K, const __nv_bfloat16* A, int64_t lda,
                   const __nv_bfloat16* B, int64_t ldb, const GemmEpilogue& ep, int k_splits, GemmWorkspace& ws);
+// The driver's cuTensorMapEncodeTiled (looked up once); throws if unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
 // Synchronises the stream and throws if a GEMM launched with ws reported a timeout.
 void gemm_check(const Exec& ex, GemmWorkspace& ws);
 

@@ -65,3 +65,60 @@ def test_spmm_empty_rows(gpu_ctx):
     x = np.arange(20, dtype=np.float64).reshape(5, 4)
     y = op.apply(torch.from_numpy(x).cuda()).cpu().numpy()
     assert np.array_equal(y, 0.5 * x + a @ x)
+
+
+_VARIANT_CACHE = {}
+
+
+def _variant_matrix():
+    """30 011 rows with ~32 entries per row (symmetrised), one empty row and one
+    row longer than a staging block; built once per session."""
+    if "a" not in _VARIANT_CACHE:
+        rng = np.random.default_rng(7)
+        n = 30_011
+        nnz = 16 * n
+        r = rng.integers(0, n, nnz)
+        c = rng.integers(0, n, nnz)
+        keep = (r != 5) & (c != 5)
+        r, c = r[keep], c[keep]
+        long_cols = rng.choice(n, 3000, replace=False)
+        long_cols = long_cols[long_cols != 5]
+        r = np.concatenate([r, np.full(long_cols.size, 17)])
+        c = np.concatenate([c, long_cols])
+        v = rng.uniform(0.1, 1.0, r.size)
+        a = sp.csr_matrix((v, (r, c)), shape=(n, n))
+        a = (a + a.T).tocsr()
+        a.sum_duplicates()
+        a.sort_indices()
+        _VARIANT_CACHE["a"] = a
+    return _VARIANT_CACHE["a"]
+
+
+@pytest.mark.parametrize("kernel", ["vec4", "vec8", "vec16", "vec32", "tiled4", "tiled8", "gather4", "gather8"])
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_spmm_every_kernel_variant(gpu_ctx, kernel, prec):
+    """Each SpMM variant the autotuner can pick (SPECTRAL_INIT_SPMM_KERNEL forces
+    one; the TMA gather4 variants apply to f32 values with 4-wide f32 blocks,
+    f64 falls back to the tuned kernel), with an empty row, a long row and the
+    implicit diagonal, against scipy in f64."""
+    import os
+    import torch
+    import spectral_init_b200 as si
+    a = _variant_matrix()
+    n = a.shape[0]
+    op = si.CsrOperator(a, diag=1.0, ctx=gpu_ctx, with_f32=(prec == "f32"))
+    dt = np.float32 if prec == "f32" else np.float64
+    x = np.random.default_rng(8).standard_normal((n, 4)).astype(dt)
+    old = os.environ.get("SPECTRAL_INIT_SPMM_KERNEL")
+    os.environ["SPECTRAL_INIT_SPMM_KERNEL"] = kernel
+    try:
+        y = op.apply(torch.from_numpy(x).cuda()).cpu().numpy()
+    finally:
+        if old is None:
+            del os.environ["SPECTRAL_INIT_SPMM_KERNEL"]
+        else:
+            os.environ["SPECTRAL_INIT_SPMM_KERNEL"] = old
+    vals = a.data.astype(np.float32).astype(np.float64) if prec == "f32" else a.data
+    av = sp.csr_matrix((vals, a.indices, a.indptr), shape=a.shape)
+    ref = x.astype(np.float64) + av @ x.astype(np.float64)
+    assert _rel(y, ref) < (2e-6 if prec == "f32" else 1e-14)
