@@ -164,6 +164,26 @@ def make_graph(a, device, rank=0):
 
 
 # ---------------------------------------------------------------------------------------------
+def dist_helpers(dist, device):
+    """(barrier, max_over_ranks) for one process per GPU; with dist None (one
+    process) both are no-ops.  Times are reduced on the device of the
+    backend (NCCL: the rank's GPU; gloo: the CPU)."""
+    import torch
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier, max_over_ranks
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -181,18 +201,22 @@ def run_ours(a):
     if world > 1:
         import torch.distributed as dist
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    def barrier():
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    barrier, max_over_ranks = dist_helpers(dist, dev)
+    try:
+        _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks)
+    finally:
         if dist is not None:
-            dist.barrier()
+            dist.destroy_process_group()
 
-    def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+
+def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
+    import numpy as np
+    import torch
+
+    import spectral_init_b200 as si
+    from spectral_init_b200 import _lib
+    from spectral_init_b200._lib import SiConfig, SiCsrF32, SiOperator, SiReport
 
     ctx = si.Context(local)
     lib = ctx.lib
