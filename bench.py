@@ -63,6 +63,9 @@ def parse_args():
                    help="the batched multi-component workload instead: 500 disconnected fuzzy-kNN components "
                         "(sizes log-uniform in [20, 100k], 1-10 clusters in 20-D), full pipeline, one JSON line")
     p.add_argument("--n-comp", type=int, default=500)
+    p.add_argument("--configs", action="store_true",
+                   help="the parity configurations instead: the n=200k family graph (FP64 / mixed / learned) and "
+                        "the n=1M graph with n_components=8 and the rSVD path; one JSON line each")
     p.add_argument("--profile-solve", action="store_true",
                    help="one FP64 and one mixed eigensolve only (after one warm-up each), for ncu launch lists")
     return p.parse_args()
@@ -576,10 +579,94 @@ def run_components(a):
     print(json.dumps(line))
 
 
+def run_configs(a):
+    """One JSON line per parity configuration (device time per solve, CUDA events)."""
+    import numpy as np
+    import torch
+    import spectral_init_b200 as si
+    from spectral_init_b200 import synthetic
+    from spectral_init_b200._lib import SiConfig, SiReport
+    from spectral_init_b200.warm_start import WEIGHTS_PATH, DeviceLaplacian, WarmStartModel
+    dev = torch.device("cuda", 0)
+    ctx = si.Context(0)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(lib.si_ctx_stream(ctx.ptr), device=dev)
+    model = None
+    if WEIGHTS_PATH.exists():
+        model = WarmStartModel.load(ctx=ctx)
+        model.attach()
+
+    def solve(lap, nc, prec=0, warm=0, level=-1, over=-1, nbiter=0):
+        cfg = SiConfig()
+        lib.si_config_default(C.byref(cfg))
+        cfg.precision, cfg.warm_start, cfg.force_level = prec, warm, level
+        cfg.rsvd_oversampling, cfg.rsvd_nbiter = over, nbiter
+        k = nc + 1
+        vals = (C.c_double * k)()
+        vecs = torch.empty(lap.n, k, dtype=torch.float64, device=dev)
+        lev = C.c_int32(-1)
+        rep = SiReport()
+        times = []
+        for _ in range(max(1, a.warmup) + max(1, a.steps)):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.check(lib.si_solve_eigenproblem(ctx.ptr, C.byref(lap.op()), nc, a.seed, lap.sqrt_deg.data_ptr(),
+                                                C.byref(cfg), vals, vecs.data_ptr(), C.byref(lev), C.byref(rep)))
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        times = times[max(1, a.warmup):]
+        return {"ms": statistics.mean(times), "iterations": rep.iterations, "level": lev.value,
+                "max_residual": rep.max_residual}, np.array(vals[:]), vecs
+
+    def sin_theta(x, y):
+        qa, _ = torch.linalg.qr(x)
+        qb, _ = torch.linalg.qr(y)
+        return float(torch.linalg.matrix_norm(qb - qa @ (qa.T @ qb), ord=2))
+
+    # n = 200k family graph: plain FP64 vs mixed vs learned start
+    n = 200_000
+    x = synthetic.gaussian_mixture_gpu(n, 30, 50, 2024, 2.0, 0.02, anisotropic=True, dirichlet_alpha=0.5, device=dev)
+    idx, dist = synthetic.knn_gpu(x, 15)
+    del x
+    sigma, rho = synthetic.smooth_knn_gpu(dist, 15)
+    g = synthetic.fuzzy_graph_gpu(idx, dist, sigma, rho)
+    del idx, dist
+    lap = DeviceLaplacian((g[0], g[1], g[2], n), ctx=ctx)
+    r64, v64, x64 = solve(lap, 2)
+    line = {"config": "n=200k: 30 anisotropic clusters (Dirichlet 0.5 sizes) in 50-D + 2% background, k=15, "
+                      "n_components=2", "nnz": lap.nnz, "fp64": r64}
+    for name, prec, warm in (("mixed", 1, 0), ("learned", 1, 1)):
+        if warm and model is None:
+            continue
+        r, v, xv = solve(lap, 2, prec, warm)
+        r["eigenvalue_abs_diff_vs_fp64"] = float(np.max(np.abs(v - v64)))
+        r["sin_theta_vs_fp64"] = sin_theta(xv[:, 1:], x64[:, 1:])
+        r["speedup_vs_fp64"] = r64["ms"] / r["ms"]
+        line[name] = r
+    line["eigengap_2_3"] = float(v64[2] - v64[1])
+    print(json.dumps(line), flush=True)
+    del lap, g
+
+    # n = 1M benchmark graph: n_components = 8, and the rSVD path (oversampling 10, 4 power iterations)
+    ip, ix, dv = make_graph(a, dev, 0)
+    lap = DeviceLaplacian((ip, ix, dv, a.n), ctx=ctx)
+    line = {"config": workload_name(a).replace(f"n_components={a.nc}", "n_components=8 and rSVD"), "nnz": lap.nnz}
+    line["lobpcg_nc8_fp64"], _, _ = solve(lap, 8)
+    line["lobpcg_nc8_mixed"], _, _ = solve(lap, 8, 1)
+    for nc in (2, 8):
+        line[f"rsvd_nc{nc}"], _, _ = solve(lap, nc, 0, 0, 4, 10, 4)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse_args()
     if a.components and a.impl == "ours":
         run_components(a)
+        return
+    if a.configs and a.impl == "ours":
+        run_configs(a)
         return
     if a.impl == "reference":
         run_reference(a)
