@@ -585,7 +585,8 @@ double mpnn_loss_backward(const Exec& ex, MpnnModel& model, const OpDev& op, Mpn
     k_transpose_bf16<<<grid, tblk, 0, ex.stream>>>(n, c, in, pin, out, npad);
     SI_LAUNCH_CHECK();
   };
-  const int ksplit = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ex.sms, (npad + 4095) / 4096)));
+  // weight gradients reduce over all n rows: split K so every SM gets a slice of at least 1024 rows
+  const int ksplit = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ex.sms, (npad + 1023) / 1024)));
 
   // ---- output layer: dW_out = A_3^T dY, db_out = colsum(dY), dA_3 = dY W_out^T
   transpose(dy.get(), kMpnnOut, kMpnnOut, dyt.get());
