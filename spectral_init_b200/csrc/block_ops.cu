@@ -281,6 +281,186 @@ __global__ void __launch_bounds__(G4_THREADS) k_gram4(const XT* __restrict__ X, 
   if (tid == 0) *counter = 0u;
 }
 
+// ---------------------------------------------------------------------------
+// Gram of one LOBPCG iteration for 8- and 16-column blocks (row width LD,
+// any m <= LD wanted columns):
+//   G1 = S^T S,  G2 = S^T AS  (upper triangles, mirrored),  S = [X R P].
+// Each 3LD x 3LD product is cut into 8 x 8 tiles of TS x TS entries
+// (TS = 3LD / 8); the 36 upper tiles of the two products are 72 register
+// tiles, one per thread of a row group.  A CTA has 7 row groups (504
+// threads: 16 warps, so 128 registers a thread fit each SM sub-partition's
+// register file); group g takes rows g, g + 7, ... of each staged 63-row
+// tile (cp.async, three stages).  The groups are added pairwise in a fixed
+// order, each CTA writes one partial per entry, and a second kernel adds the
+// CTAs' partials in CTA order (a wide reduction instead of one finishing
+// CTA).
+template <int LD>
+struct GramLd {
+  static constexpr int TS = 3 * LD / 8;
+  static constexpr int W = 6 * LD;  // staged row: X R P AX AR AP
+  static constexpr int TILES = 72;
+  static constexpr int GROUPS = 7;
+  static constexpr int THREADS = TILES * GROUPS;  // 504
+  static constexpr int TR = 63;                   // rows per stage (9 per group)
+  static constexpr int STAGES = 3;
+  static constexpr int ENTRIES = TILES * TS * TS;  // partials per CTA
+};
+template <class XT, int LD>
+__host__ __device__ constexpr int gram_ld_stride() {
+  return GramLd<LD>::W + static_cast<int>(16 / sizeof(XT));  // padded row, 16-byte multiple
+}
+template <class XT, int LD>
+constexpr size_t gram_ld_smem() {
+  using C = GramLd<LD>;
+  const size_t stages = static_cast<size_t>(C::STAGES) * C::TR * gram_ld_stride<XT, LD>() * sizeof(XT);
+  const size_t red = static_cast<size_t>(C::GROUPS - C::GROUPS / 2) * C::ENTRIES * sizeof(double);
+  return stages > red ? stages : red;
+}
+
+// upper tile u in [0, 36) of an 8 x 8 tile grid -> (ti, tj), ti <= tj
+__device__ __forceinline__ void upper_tile(int u, int& ti, int& tj) {
+  ti = 0;
+  while (u >= 8 - ti) {
+    u -= 8 - ti;
+    ++ti;
+  }
+  tj = ti + u;
+}
+
+template <class XT, int LD>
+__global__ void __maxnreg__(128)
+    k_gram_ld(const XT* __restrict__ X, const XT* __restrict__ R, const XT* __restrict__ P,
+              const XT* __restrict__ AX, const XT* __restrict__ AR, const XT* __restrict__ AP, int64_t n,
+              double* __restrict__ partial, const int* __restrict__ stop) {
+  using C = GramLd<LD>;
+  constexpr int TS = C::TS, SW = gram_ld_stride<XT, LD>();
+  if (stop != nullptr && *stop != 0) return;
+  extern __shared__ __align__(16) unsigned char gram_ld_raw[];
+  XT* tile = reinterpret_cast<XT*>(gram_ld_raw);
+  double* red = reinterpret_cast<double*>(gram_ld_raw);
+  const int tid = threadIdx.x;
+  const int g = tid / C::TILES, tau = tid % C::TILES;
+  const int h = tau / 36;
+  int ti, tj;
+  upper_tile(tau % 36, ti, tj);
+  const int sb = ti * TS;                  // S columns sb .. sb + TS - 1
+  const int tb = h * 3 * LD + tj * TS;     // T = [S AS] columns
+  double acc[TS][TS];
+#pragma unroll
+  for (int p = 0; p < TS; ++p)
+#pragma unroll
+    for (int q = 0; q < TS; ++q) acc[p][q] = 0.0;
+  constexpr int EPC = 16 / sizeof(XT);       // elements per 16-byte chunk
+  constexpr int CPB = LD / EPC;              // chunks per (row, block)
+  constexpr int NCH = C::TR * 6 * CPB;
+  const int64_t ntiles = (n + C::TR - 1) / C::TR;
+  auto load_tile = [&](int64_t t, int buf) {
+    if (t < ntiles) {
+      const int64_t row0 = t * C::TR;
+      for (int c = tid; c < NCH; c += C::THREADS) {
+        const int b = c / (C::TR * CPB);
+        const int rem = c % (C::TR * CPB);
+        const int r = rem / CPB, hh = rem % CPB;
+        const int64_t row = row0 + r;
+        const bool ok = row < n;
+        const XT* base = b < 3 ? (b == 0 ? X : (b == 1 ? R : P)) : (b == 3 ? AX : (b == 4 ? AR : AP));
+        cp_async16(tile + (static_cast<size_t>(buf) * C::TR + r) * SW + b * LD + hh * EPC,
+                   base + (ok ? row : 0) * LD + hh * EPC, ok ? 16 : 0);
+      }
+    }
+    cp_async_commit();  // empty groups keep the group count uniform
+  };
+  const int64_t step = gridDim.x;
+  int64_t t = blockIdx.x;
+#pragma unroll
+  for (int s0 = 0; s0 < C::STAGES - 1; ++s0) load_tile(t + s0 * step, s0);
+  int buf = 0;
+  for (; t < ntiles; t += step) {
+    load_tile(t + (C::STAGES - 1) * step, (buf + C::STAGES - 1) % C::STAGES);
+    cp_async_wait<C::STAGES - 1>();
+    __syncthreads();
+#pragma unroll 2
+    for (int r = g; r < C::TR; r += C::GROUPS) {
+      const XT* row = tile + (static_cast<size_t>(buf) * C::TR + r) * SW;
+      double s[TS];
+#pragma unroll
+      for (int p = 0; p < TS; ++p) s[p] = static_cast<double>(row[sb + p]);
+#pragma unroll
+      for (int q = 0; q < TS; ++q) {
+        const double tv = static_cast<double>(row[tb + q]);
+#pragma unroll
+        for (int p = 0; p < TS; ++p) acc[p][q] = fma(s[p], tv, acc[p][q]);
+      }
+    }
+    __syncthreads();
+    buf = (buf + 1) % C::STAGES;
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  // row groups added pairwise: g += g + 4, then g + 2, then g + 1
+  const int e0 = tau * TS * TS;
+#pragma unroll
+  for (int half = 4; half >= 1; half >>= 1) {
+    if (g >= half && g < 2 * half) {
+#pragma unroll
+      for (int p = 0; p < TS; ++p)
+#pragma unroll
+        for (int q = 0; q < TS; ++q) red[(g - half) * C::ENTRIES + e0 + p * TS + q] = acc[p][q];
+    }
+    __syncthreads();
+    if (g < half && g + half < C::GROUPS) {
+#pragma unroll
+      for (int p = 0; p < TS; ++p)
+#pragma unroll
+        for (int q = 0; q < TS; ++q) acc[p][q] += red[g * C::ENTRIES + e0 + p * TS + q];
+    }
+    __syncthreads();
+  }
+  if (g == 0) {
+    double* dst = partial + static_cast<int64_t>(blockIdx.x) * C::ENTRIES + e0;
+#pragma unroll
+    for (int p = 0; p < TS; ++p)
+#pragma unroll
+      for (int q = 0; q < TS; ++q) dst[p * TS + q] = acc[p][q];
+  }
+}
+
+// Adds the per-CTA partials of k_gram_ld in CTA order and writes both
+// (3m) x (3m) matrices.  A CTA takes 32 entries: warp w adds CTAs w, w + 8,
+// ..., then the eight warp sums are added in warp order.
+template <int LD>
+__global__ void __launch_bounds__(256) k_gram_ld_reduce(const double* __restrict__ partial, int nparts, int m,
+                                                        double* __restrict__ out, const int* __restrict__ stop) {
+  using C = GramLd<LD>;
+  constexpr int TS = C::TS;
+  if (stop != nullptr && *stop != 0) return;
+  __shared__ double red[8][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int e = blockIdx.x * 32 + lane;
+  double s = 0.0;
+  if (e < C::ENTRIES)
+    for (int c = warp; c < nparts; c += 8) s += partial[static_cast<int64_t>(c) * C::ENTRIES + e];
+  red[warp][lane] = s;
+  __syncthreads();
+  if (warp != 0 || e >= C::ENTRIES) return;
+  double v = 0.0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) v += red[w][lane];
+  const int tau = e / (TS * TS), pq = e % (TS * TS), p = pq / TS, q = pq % TS;
+  const int h = tau / 36;
+  int ti, tj;
+  upper_tile(tau % 36, ti, tj);
+  if (ti == tj && p > q) return;  // lower half of a diagonal tile
+  const int i = ti * TS + p, j = tj * TS + q;  // entry (i, j) of the 3LD x 3LD product, i <= j
+  const int ci = i % LD, cj = j % LD;
+  if (ci >= m || cj >= m) return;
+  const int P = 3 * m;
+  const int I = (i / LD) * m + ci, J = (j / LD) * m + cj;
+  double* o = out + h * P * P;
+  o[I * P + J] = v;
+  o[J * P + I] = v;
+}
+
 // LOBPCG update with 4-column blocks: four threads per row, thread j produces
 // output column j (inputs are read as 4-vectors; the four threads of a row
 // share the same sectors).
@@ -785,6 +965,107 @@ __global__ void __launch_bounds__(256) k_lobpcg_update(LobpcgBlocks<XT> b, const
   }
 }
 
+// 16-byte vector of XT
+template <class XT>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using type = double2;
+};
+template <>
+struct Vec16<float> {
+  using type = float4;
+};
+
+// LOBPCG update for 8- and 16-column blocks: LD / 4 threads per row, each
+// producing four output columns from the whole input rows (16-byte loads; the
+// threads of a row share the sectors), coefficients from shared memory
+// (zero outside the m x m block).  Same formulas as k_lobpcg_update.
+template <class XT, int LD>
+__global__ void __launch_bounds__(256) k_lobpcg_update_q(LobpcgBlocks<XT> b, const LobpcgCtrl* __restrict__ ctrl,
+                                                         int64_t n, int init_mode) {
+  constexpr int TPR = LD / 4;
+  constexpr int EPV = 16 / sizeof(XT);  // elements per 16-byte load
+  using V = typename Vec16<XT>::type;
+  __shared__ __align__(16) double sC[3][LD][LD];
+  __shared__ double sLam[LD];
+  const int done = ctrl->done, copy_best = ctrl->copy_best, use_p = ctrl->has_p, m = ctrl->m;
+  if (done && !copy_best) return;
+  for (int i = threadIdx.x; i < 3 * LD * LD; i += blockDim.x) {
+    const int w = i / (LD * LD), r = (i / LD) % LD, c = i % LD;
+    const double* src = w == 0 ? ctrl->Cx : (w == 1 ? ctrl->Cr : ctrl->Cp);
+    sC[w][r][c] = (r < m && c < m) ? src[r * MAXM + c] : 0.0;
+  }
+  if (threadIdx.x < LD) sLam[threadIdx.x] = static_cast<int>(threadIdx.x) < m ? ctrl->lam[threadIdx.x] : 0.0;
+  __syncthreads();
+  const int64_t total = n * TPR;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;  // multiple of 32
+  // the loop condition uses the warp's base index, so all lanes of a warp run
+  // the same trip count and reach the __syncwarp below together
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; (t & ~int64_t(31)) < total;
+       t += stride) {
+    const bool valid = t < total;  // a row's TPR lanes agree
+    const int64_t i = valid ? t / TPR : 0;
+    const int j0 = static_cast<int>(t % TPR) * 4;
+    const int64_t o = i * LD;
+    if (valid && copy_best) {
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) b.Xbest[o + j0 + jj] = b.X[o + j0 + jj];
+    }
+    if (done) continue;  // uniform
+    double xn[4] = {0.0, 0.0, 0.0, 0.0}, axn[4] = {0.0, 0.0, 0.0, 0.0};
+    double pn[4] = {0.0, 0.0, 0.0, 0.0}, apn[4] = {0.0, 0.0, 0.0, 0.0};
+    // out[jj] += sum_c in_a[c] C[c][j0 + jj], out2[jj] += sum_c in_b[c] C[c][j0 + jj]
+    auto accumulate = [&](const XT* ina, const XT* inb, int w, double* outa, double* outb) {
+#pragma unroll
+      for (int c0 = 0; c0 < LD; c0 += EPV) {
+        XT va[EPV], vb[EPV];
+        *reinterpret_cast<V*>(va) = *reinterpret_cast<const V*>(ina + o + c0);
+        *reinterpret_cast<V*>(vb) = *reinterpret_cast<const V*>(inb + o + c0);
+#pragma unroll
+        for (int cc = 0; cc < EPV; ++cc) {
+          const double a = static_cast<double>(va[cc]), bb = static_cast<double>(vb[cc]);
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const double cf = sC[w][c0 + cc][j0 + jj];
+            outa[jj] = fma(a, cf, outa[jj]);
+            outb[jj] = fma(bb, cf, outb[jj]);
+          }
+        }
+      }
+    };
+    if (!init_mode) {
+      accumulate(b.R, b.AR, 1, pn, apn);
+      if (use_p) accumulate(b.P, b.AP, 2, pn, apn);
+    }
+    accumulate(b.X, b.AX, 0, xn, axn);
+    // every thread of the row has read its inputs before any column is overwritten
+    __syncwarp();
+    if (!valid) continue;
+    XT xs[4], axs[4], rs[4], ps[4], aps[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int j = j0 + jj;
+      const bool active = j < m;
+      xs[jj] = static_cast<XT>(active ? xn[jj] + pn[jj] : 0.0);
+      axs[jj] = static_cast<XT>(active ? axn[jj] + apn[jj] : 0.0);
+      rs[jj] = static_cast<XT>(active ? static_cast<double>(axs[jj]) - sLam[j] * static_cast<double>(xs[jj]) : 0.0);
+      ps[jj] = static_cast<XT>(active ? pn[jj] : 0.0);
+      aps[jj] = static_cast<XT>(active ? apn[jj] : 0.0);
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      b.X[o + j0 + jj] = xs[jj];
+      b.AX[o + j0 + jj] = axs[jj];
+      b.R[o + j0 + jj] = rs[jj];
+      if (!init_mode) {
+        b.P[o + j0 + jj] = ps[jj];
+        b.AP[o + j0 + jj] = aps[jj];
+      }
+    }
+  }
+}
+
 // Generic update for any ld (column loop, reads straight from global).
 template <class XT>
 __global__ void __launch_bounds__(256) k_lobpcg_update_generic(LobpcgBlocks<XT> b, const LobpcgCtrl* __restrict__ ctrl,
@@ -873,12 +1154,46 @@ int grid_rows(const Exec& ex, int64_t items, int threads = 256, int per_sm = 8) 
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(ex.sms) * per_sm)));
 }
 
+template <class XT, int LD>
+void gram_ld_launch(const Exec& ex, GramWork& w, const XT* const* blk, int m, int64_t n, double* out,
+                    const int* stop) {
+  using C = GramLd<LD>;
+  constexpr size_t smem = gram_ld_smem<XT, LD>();
+  // resident CTAs per SM (set once per device)
+  static std::atomic<int> resident[64];
+  SI_REQUIRE(ex.device >= 0 && ex.device < 64, SI_INVALID_ARGUMENT, "gram: device ordinal");
+  if (resident[ex.device] == 0) {
+    SI_CUDA(cudaFuncSetAttribute(k_gram_ld<XT, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    int r = 0;
+    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gram_ld<XT, LD>, C::THREADS, smem));
+    resident[ex.device] = std::max(1, r);
+  }
+  const int64_t ntiles = (n + C::TR - 1) / C::TR;
+  const int grid = static_cast<int>(
+      std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ex.sms) * resident[ex.device].load())));
+  w.ensure(static_cast<size_t>(grid) * C::ENTRIES, ex.stream);
+  k_gram_ld<XT, LD><<<grid, C::THREADS, smem, ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4], blk[5], n,
+                                                           w.partial.get(), stop);
+  SI_LAUNCH_CHECK();
+  k_gram_ld_reduce<LD><<<(C::ENTRIES + 31) / 32, 256, 0, ex.stream>>>(w.partial.get(), grid, m, out, stop);
+  SI_LAUNCH_CHECK();
+}
+
 }  // namespace
 
 template <class XT>
 void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, int ns, int nblk, int m, int ld,
               int64_t n, double* out, const int* stop) {
   SI_REQUIRE(nblk >= 1 && nblk <= 8 && m >= 1 && nblk * m <= GMAXW, SI_INVALID_ARGUMENT, "gram: too many columns");
+  if (mode == GRAM_SYM2 && ns == 3 && nblk == 6 && m <= ld && (ld == 8 || ld == 16)) {
+    // the per-iteration LOBPCG Gram of 8- and 16-column blocks
+    if (ld == 8)
+      gram_ld_launch<XT, 8>(ex, w, blk, m, n, out, stop);
+    else
+      gram_ld_launch<XT, 16>(ex, w, blk, m, n, out, stop);
+    return;
+  }
   if (mode == GRAM_SYM2 && ns == 3 && nblk == 6 && m == 4 && ld == 4) {
     // the per-iteration LOBPCG Gram of 4-column blocks
     // resident CTAs per SM from the stage memory (set once per device)
@@ -1044,7 +1359,9 @@ void lobpcg_update_dev(const Exec& ex, const LobpcgBlocks<XT>& b, const LobpcgCt
   if (ld == 4)
     k_lobpcg_update4<XT><<<grid_rows(ex, n * 4), 256, 0, ex.stream>>>(b, ctrl, n, init_mode);
   else if (ld == 8)
-    k_lobpcg_update<XT, 8><<<grid, 256, 0, ex.stream>>>(b, ctrl, n, init_mode);
+    k_lobpcg_update_q<XT, 8><<<grid_rows(ex, n * 2), 256, 0, ex.stream>>>(b, ctrl, n, init_mode);
+  else if (ld == 16)
+    k_lobpcg_update_q<XT, 16><<<grid_rows(ex, n * 4), 256, 0, ex.stream>>>(b, ctrl, n, init_mode);
   else
     k_lobpcg_update_generic<XT><<<grid, 256, 0, ex.stream>>>(b, ctrl, n, ld, init_mode);
   SI_LAUNCH_CHECK();

@@ -2,8 +2,10 @@
 // (dense_evd, src/solvers/dense.rs:9-46; Levels 0 and 5 of the chain).
 //
 //   1. densify the operator (lower triangle mirrored, like faer's Side::Lower);
-//   2. Householder tridiagonalisation T = Q^T A Q (dsytd2-style, one CTA,
-//      matrix resident in L2 for n <= 2000);
+//   2. Householder tridiagonalisation T = Q^T A Q (dsytd2-style): one CTA
+//      below 192 rows, one cooperative launch with the matrix spread over the
+//      shared memory of co-resident CTAs up to 2048 rows, and three launches
+//      per column above that;
 //   3. split T where off-diagonals are negligible, then for every block the
 //      smallest eigenvalues by Sturm-count bisection; the k smallest overall
 //      are kept;
@@ -11,7 +13,12 @@
 //      partial pivoting of T - lambda I), re-orthogonalised within clusters of
 //      close eigenvalues (modified Gram-Schmidt);
 //   5. back-transformation v = Q y with the stored reflectors.
+#include <algorithm>
 #include <cfloat>
+#include <cmath>
+#include <cstdlib>
+#include <mutex>
+#include <string>
 
 #include "si_internal.h"
 
@@ -19,6 +26,7 @@ namespace si {
 namespace {
 
 constexpr int DT = 1024;
+constexpr int TE_MS_ITEMS = 32;  // multisection when at most this many (block, index) items
 constexpr int64_t kTriMultiMin = 192;  // from this n the tridiagonalisation runs as multi-CTA steps
 
 __global__ void k_densify(int64_t n, const uint64_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
@@ -229,6 +237,214 @@ __global__ void k_tri_last(const double* A, int n, double* d, double* e, double*
   d[n - 1] = A[static_cast<int64_t>(n - 1) * n + n - 1];
 }
 
+// ---- single-launch tridiagonalisation (kTriMultiMin <= n <= kTriCoopMax) ----
+// The same Householder steps with the matrix held in the shared memory of G
+// co-resident CTAs (cooperative launch): row r lives in CTA r % G, slot r / G,
+// so a step touches on-chip data plus two n-vectors in L2.  Step j:
+//   (1) the CTA holding row j forms the reflector from that row (A is kept
+//       exactly symmetric, so row j equals column j), writes v, d, e, tau and
+//       the reflector (row j of A in global memory) and publishes the step
+//       with a release store;
+//   (2) every CTA computes w_r = tau (A v)_r for its rows r > j and its share
+//       of w.v; grid barrier;
+//   (3) every CTA adds the shares in CTA order, K = tau (w.v) / 2,
+//       w' = w - K v, and updates its rows A -= v w'^T + w' v^T, each entry
+//       as round(v_r w'_c) + round(w'_r v_c) so entries (r, c) and (c, r)
+//       stay identical.
+// v, w and the shares are double-buffered by step parity: a buffer is written
+// again two steps later, after a barrier that all of its readers have passed.
+// Every wait is bounded: a CTA that waits longer than the limit sets the error
+// word, every CTA returns, and the host redoes the matrix with the
+// multi-launch steps.
+constexpr int CT_THREADS = 512;
+constexpr int CT_RMAX = 16;                                    // rows per CTA
+constexpr int CT_CMAX = 4;                                     // columns per thread
+constexpr int64_t kTriCoopMax = int64_t(CT_THREADS) * CT_CMAX;  // 2048
+constexpr uint64_t kCoopWaitNs = 2000000000ull;                // 2 s per wait
+
+struct CoopTri {
+  double* A;  // n x n, exactly symmetric on entry; reflector of step j goes to row j
+  int n, G, R;
+  double *d, *e, *tau;
+  double* vbuf;      // [2][n]
+  double* wbuf;      // [2][n]
+  double* share;     // [2][G]
+  unsigned* vready;  // last step whose reflector is published
+  unsigned* arrive;  // grid barrier arrivals (G per step)
+  int* err;
+};
+
+__device__ __forceinline__ uint64_t coop_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// One thread: wait until *p >= target.  False when the wait ran past the limit
+// (the error word is set) or another CTA gave up first.
+__device__ bool coop_wait(const unsigned* p, unsigned target, int* err) {
+  if (ld_acquire_u32(p) >= target) return true;
+  const uint64_t t0 = coop_ns();
+  while (ld_acquire_u32(p) < target) {
+    if (*reinterpret_cast<volatile int*>(err) != 0) return false;
+    if (coop_ns() - t0 > kCoopWaitNs) {
+      atomicExch(err, 1);
+      return false;
+    }
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(CT_THREADS, 1) k_tridiag_coop(CoopTri p) {
+  extern __shared__ double rows[];  // [R][n]
+  __shared__ double red[CT_THREADS / 32][CT_RMAX];
+  __shared__ double s_v[CT_RMAX], s_w[CT_RMAX];
+  __shared__ double s_scal, s_K;
+  __shared__ int s_ok;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n = p.n, G = p.G, R = p.R, b = blockIdx.x;
+  for (int l = 0; l < R; ++l) {
+    const int r = l * G + b;
+    if (r >= n) break;
+    for (int c = tid; c < n; c += CT_THREADS) rows[l * n + c] = p.A[static_cast<int64_t>(r) * n + c];
+  }
+  __syncthreads();
+  for (int j = 0; j + 2 < n; ++j) {
+    const int par = j & 1;
+    double* vb = p.vbuf + par * n;
+    double* wb = p.wbuf + par * n;
+    double* sh = p.share + par * G;
+    // (1) reflector of row j
+    if (j % G == b) {
+      const double* rj = rows + (j / G) * n;
+      double part = 0.0;
+      for (int i = j + 2 + tid; i < n; i += CT_THREADS) part = fma(rj[i], rj[i], part);
+      const double sigma = block_sum_all(part, &red[0][0]);
+      if (tid == 0) {
+        const double alpha = rj[j + 1];
+        double t = 0.0, beta = alpha, scal = 0.0;
+        if (sigma > 0.0) {
+          const double nrm = sqrt(alpha * alpha + sigma);
+          beta = alpha >= 0.0 ? -nrm : nrm;
+          t = (beta - alpha) / beta;
+          scal = 1.0 / (alpha - beta);
+        }
+        s_scal = scal;
+        p.d[j] = rj[j];
+        p.e[j] = beta;
+        p.tau[j] = t;
+      }
+      __syncthreads();
+      const double scal = s_scal;
+      for (int i = j + 1 + tid; i < n; i += CT_THREADS) {
+        const double vi = (i == j + 1) ? 1.0 : rj[i] * scal;
+        vb[i] = vi;
+        if (i >= j + 2) p.A[static_cast<int64_t>(j) * n + i] = vi;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        st_release_u32(p.vready, static_cast<unsigned>(j + 1));
+      }
+    }
+    if (tid == 0) s_ok = coop_wait(p.vready, static_cast<unsigned>(j + 1), p.err) ? 1 : 0;
+    __syncthreads();
+    if (!s_ok) return;
+    const double tau = __ldcg(p.tau + j);
+    // (2) w = tau A v on this CTA's rows r > j
+    // slots below l0 hold finished rows (r <= j)
+    const int l0 = j >= b ? (j - b) / G + 1 : 0;
+    double vc[CT_CMAX], acc[CT_RMAX];
+#pragma unroll
+    for (int l = 0; l < CT_RMAX; ++l) acc[l] = 0.0;
+#pragma unroll
+    for (int q = 0; q < CT_CMAX; ++q) {
+      const int c = j + 1 + tid + q * CT_THREADS;
+      vc[q] = c < n ? __ldcg(vb + c) : 0.0;
+      if (c < n) {
+#pragma unroll
+        for (int l = 0; l < CT_RMAX; ++l)
+          if (l >= l0 && l < R) acc[l] = fma(rows[l * n + c], vc[q], acc[l]);
+      }
+    }
+#pragma unroll
+    for (int l = 0; l < CT_RMAX; ++l) {
+      if (l >= l0 && l < R) {
+        const double s = warp_sum(acc[l]);
+        if (lane == 0) red[warp][l] = s;
+      }
+    }
+    __syncthreads();
+    if (tid < R) {
+      const int r = tid * G + b;
+      if (r > j && r < n) {
+        double s = 0.0;
+        for (int w = 0; w < CT_THREADS / 32; ++w) s += red[w][tid];
+        const double wr = tau * s;
+        wb[r] = wr;
+        s_w[tid] = wr;
+        s_v[tid] = __ldcg(vb + r);
+      } else {
+        s_w[tid] = 0.0;
+        s_v[tid] = 0.0;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int l = 0; l < R; ++l) s = fma(s_w[l], s_v[l], s);
+      sh[b] = s;
+      __threadfence();
+      atomicAdd(p.arrive, 1u);
+      s_ok = coop_wait(p.arrive, static_cast<unsigned>(j + 1) * static_cast<unsigned>(G), p.err) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    // (3) K, w' and the rank-2 update of this CTA's rows
+    if (warp == 0) {
+      double s = 0.0;
+      for (int c = lane; c < G; c += 32) s += __ldcg(sh + c);
+      s = warp_sum(s);
+      if (lane == 0) s_K = 0.5 * tau * s;
+    }
+    __syncthreads();
+    const double K = s_K;
+#pragma unroll
+    for (int q = 0; q < CT_CMAX; ++q) {
+      const int c = j + 1 + tid + q * CT_THREADS;
+      if (c < n) {
+        const double wc = fma(-K, vc[q], __ldcg(wb + c));
+#pragma unroll
+        for (int l = 0; l < CT_RMAX; ++l) {
+          if (l >= l0 && l < R && l * G + b < n) {
+            const double wr = fma(-K, s_v[l], s_w[l]);
+            const double u = __dadd_rn(__dmul_rn(s_v[l], wc), __dmul_rn(wr, vc[q]));
+            rows[l * n + c] -= u;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0 && n >= 2) {
+    const int r2 = n - 2, r1 = n - 1;
+    if (r2 % G == b) {
+      const double* row = rows + (r2 / G) * n;
+      p.d[r2] = row[r2];
+      p.e[r2] = row[r1];
+      p.tau[r2] = 0.0;
+    }
+    if (r1 % G == b) p.d[r1] = rows[(r1 / G) * n + r1];
+  }
+}
+
 // number of eigenvalues of T[l..r] smaller than x (Sturm sequence)
 __device__ int sturm_count(const double* d, const double* e, int l, int r, double x, double pivmin) {
   int cnt = 0;
@@ -285,16 +501,21 @@ __global__ void __launch_bounds__(DT) k_tri_eig(const double* __restrict__ d, co
   const int nb = s_nb;
   const double tnorm = s_tnorm;
   const double pivmin = fmax(DBL_MIN, tnorm * tnorm * DBL_MIN);
-  // bisection for (block, index) items
-  for (int q = tid; q < nb * k; q += blockDim.x) {
+  // absolute tolerance of the eigenvalue intervals: eps |T| (the default of
+  // LAPACK's dstebz); relative eps for eigenvalues away from zero
+  const double atol = DBL_EPSILON * tnorm + pivmin;
+  const int nitems = nb * k;
+  // Gershgorin interval of item q's block; false if the block has no t-th eigenvalue
+  auto item_interval = [&](int q, double& lo, double& hi) {
     const int b = q / k, t = q % k;
     const int l = w.bstart[b], r = w.bstart[b + 1] - 1;
+    w.cand_blk[q] = b;
     if (t > r - l) {
       w.cand[q] = DBL_MAX;
-      w.cand_blk[q] = b;
-      continue;
+      return false;
     }
-    double lo = DBL_MAX, hi = -DBL_MAX;
+    lo = DBL_MAX;
+    hi = -DBL_MAX;
     for (int i = l; i <= r; ++i) {
       const double rad = (i > l ? fabs(w.es[i - 1]) : 0.0) + (i < r ? fabs(w.es[i]) : 0.0);
       lo = fmin(lo, d[i] - rad);
@@ -302,13 +523,71 @@ __global__ void __launch_bounds__(DT) k_tri_eig(const double* __restrict__ d, co
     }
     lo -= 2.0 * DBL_EPSILON * tnorm + pivmin;
     hi += 2.0 * DBL_EPSILON * tnorm + pivmin;
-    for (int it = 0; it < 200; ++it) {
-      const double mid = 0.5 * (lo + hi);
-      if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin || mid == lo || mid == hi) break;
-      if (sturm_count(d, w.es, l, r, mid, pivmin) > t) hi = mid; else lo = mid;
+    return true;
+  };
+  auto converged = [&](double lo, double hi) {
+    const double mid = 0.5 * (lo + hi);
+    return hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + atol || mid == lo || mid == hi;
+  };
+  if (nitems <= TE_MS_ITEMS) {
+    // multisection: the P threads of an item count eigenvalues below P interior
+    // points of its interval per round, and the interval shrinks to the gap
+    // between the two points around the wanted index (a factor P + 1 a round)
+    __shared__ double s_lo[TE_MS_ITEMS], s_hi[TE_MS_ITEMS];
+    __shared__ int s_live[TE_MS_ITEMS];
+    __shared__ int s_cnt[DT];
+    const int P = static_cast<int>(blockDim.x) / nitems;
+    if (tid < nitems) {
+      double lo = 0.0, hi = 0.0;
+      const bool ok = item_interval(tid, lo, hi);
+      s_lo[tid] = lo;
+      s_hi[tid] = hi;
+      s_live[tid] = ok && !converged(lo, hi);
+      if (ok && !s_live[tid]) w.cand[tid] = 0.5 * (lo + hi);
     }
-    w.cand[q] = 0.5 * (lo + hi);
-    w.cand_blk[q] = b;
+    __syncthreads();
+    const int item = tid / P, pi = tid % P;
+    auto point = [&](double lo, double hi, int p) { return lo + (hi - lo) * (static_cast<double>(p + 1) / (P + 1)); };
+    for (int round = 0; round < 200; ++round) {
+      if (item < nitems && s_live[item]) {
+        const int b = item / k;
+        s_cnt[tid] = sturm_count(d, w.es, w.bstart[b], w.bstart[b + 1] - 1, point(s_lo[item], s_hi[item], pi), pivmin);
+      }
+      __syncthreads();
+      int more = 0;
+      if (tid < nitems && s_live[tid]) {
+        const int t = tid % k;
+        const double lo = s_lo[tid], hi = s_hi[tid];
+        int p = 0;
+        while (p < P && s_cnt[tid * P + p] <= t) ++p;
+        // count(point p - 1) <= t < count(point p)
+        const double nlo = p == 0 ? lo : point(lo, hi, p - 1);
+        const double nhi = p == P ? hi : point(lo, hi, p);
+        s_lo[tid] = nlo;
+        s_hi[tid] = nhi;
+        if (converged(nlo, nhi) || (nlo == lo && nhi == hi)) {
+          s_live[tid] = 0;
+          w.cand[tid] = 0.5 * (nlo + nhi);
+        } else {
+          more = 1;
+        }
+      }
+      if (!__syncthreads_or(more)) break;
+    }
+    if (tid < nitems && s_live[tid]) w.cand[tid] = 0.5 * (s_lo[tid] + s_hi[tid]);
+  } else {
+    // one thread per item, bisection
+    for (int q = tid; q < nitems; q += blockDim.x) {
+      double lo = 0.0, hi = 0.0;
+      if (!item_interval(q, lo, hi)) continue;
+      const int b = q / k, t = q % k;
+      const int l = w.bstart[b], r = w.bstart[b + 1] - 1;
+      for (int it = 0; it < 200 && !converged(lo, hi); ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (sturm_count(d, w.es, l, r, mid, pivmin) > t) hi = mid; else lo = mid;
+      }
+      w.cand[q] = 0.5 * (lo + hi);
+    }
   }
   __syncthreads();
   if (tid != 0) return;
@@ -447,6 +726,206 @@ __global__ void __launch_bounds__(DT) k_backtransform(const double* __restrict__
   }
 }
 
+// The same product with Y (n x k) in shared memory: each of the 256 threads
+// owns rows tid, tid + 256, ... (at most BT_RPT), so the only exchange per
+// reflector is the k dot products (warp sums, then the eight warp partials in
+// warp order; double-buffered, one barrier per reflector).  The reflector of
+// the next step is loaded while the current one is applied.
+constexpr int BT_THREADS = 256;
+constexpr int BT_RPT = 8;  // rows per thread: n <= 2048
+
+__global__ void __launch_bounds__(BT_THREADS) k_backtransform_smem(const double* __restrict__ A,
+                                                                   const double* __restrict__ tau, int n,
+                                                                   double* __restrict__ Y, int ld, int k) {
+  extern __shared__ double ys[];  // [n][k]
+  __shared__ double red[2][BT_THREADS / 32][MAXM];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int idx = tid; idx < n * k; idx += BT_THREADS) ys[idx] = Y[static_cast<int64_t>(idx / k) * ld + idx % k];
+  // u of reflector j on this thread's rows (zero outside rows j + 1 .. n - 1)
+  auto load_u = [&](int j, double* u) {
+#pragma unroll
+    for (int q = 0; q < BT_RPT; ++q) {
+      const int r = tid + q * BT_THREADS;
+      u[q] = r == j + 1 ? 1.0 : ((r > j + 1 && r < n) ? A[static_cast<int64_t>(j) * n + r] : 0.0);
+    }
+  };
+  double u[BT_RPT], un[BT_RPT];
+  load_u(n - 3, u);
+  __syncthreads();
+  int buf = 0;
+  for (int j = n - 3; j >= 0; --j) {
+    const double t = tau[j];
+    if (j > 0) load_u(j - 1, un);
+    if (t != 0.0) {
+      double part[MAXM];
+#pragma unroll
+      for (int v = 0; v < MAXM; ++v) part[v] = 0.0;
+#pragma unroll
+      for (int q = 0; q < BT_RPT; ++q) {
+        const int r = tid + q * BT_THREADS;
+        if (r > j && r < n) {
+#pragma unroll
+          for (int v = 0; v < MAXM; ++v)
+            if (v < k) part[v] = fma(u[q], ys[r * k + v], part[v]);
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < MAXM; ++v) {
+        if (v < k) {
+          const double s = warp_sum(part[v]);
+          if (lane == 0) red[buf][warp][v] = s;
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int v = 0; v < MAXM; ++v) {
+        if (v < k) {
+          double dsum = 0.0;
+#pragma unroll
+          for (int w = 0; w < BT_THREADS / 32; ++w) dsum += red[buf][w][v];
+          const double dv = t * dsum;
+#pragma unroll
+          for (int q = 0; q < BT_RPT; ++q) {
+            const int r = tid + q * BT_THREADS;
+            if (r > j && r < n) ys[r * k + v] -= dv * u[q];
+          }
+        }
+      }
+      buf ^= 1;
+    }
+#pragma unroll
+    for (int q = 0; q < BT_RPT; ++q) u[q] = un[q];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < n * k; idx += BT_THREADS) Y[static_cast<int64_t>(idx / k) * ld + idx % k] = ys[idx];
+}
+
+}  // namespace
+
+namespace {
+
+void densify(const Exec& ex, const OpDev& op, double* A) {
+  const int64_t n = op.n;
+  SI_CUDA(cudaMemsetAsync(A, 0, sizeof(double) * n * n, ex.stream));
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, int64_t(ex.sms) * 8)));
+  k_densify<<<grid, 256, 0, ex.stream>>>(n, op.indptr, op.indices, op.v64, op.diag, A);
+  SI_LAUNCH_CHECK();
+  k_mirror_lower<<<static_cast<int>(std::min<int64_t>((n * n + 255) / 256, int64_t(ex.sms) * 16)), 256, 0,
+                   ex.stream>>>(n, A);
+  SI_LAUNCH_CHECK();
+}
+
+// The multi-launch steps (three launches per column).
+void tridiag_steps(const Exec& ex, double* A, int n, double* d, double* e, double* tau) {
+  DevBuf<double> vbuf(n, ex.stream), wbuf(n, ex.stream), partial((n + 7) / 8, ex.stream);
+  DevBuf<unsigned> counter(1, ex.stream);
+  counter.zero();
+  for (int j = 0; j + 2 < n; ++j) {
+    const int len = n - j - 1;
+    k_tri_house<<<1, 256, 0, ex.stream>>>(A, n, j, d, e, tau, vbuf.get());
+    SI_LAUNCH_CHECK();
+    k_tri_matvec<<<(len + 7) / 8, 256, 0, ex.stream>>>(A, n, j, tau, vbuf.get(), wbuf.get(), partial.get(),
+                                                       counter.get());
+    SI_LAUNCH_CHECK();
+    k_tri_update<<<std::min(len, ex.sms * 8), 256, 0, ex.stream>>>(A, n, j, tau, vbuf.get(), wbuf.get());
+    SI_LAUNCH_CHECK();
+  }
+  k_tri_last<<<1, 32, 0, ex.stream>>>(A, n, d, e, tau);
+  SI_LAUNCH_CHECK();
+}
+
+// Per-device limits of the single-launch tridiagonalisation.
+struct CoopLimits {
+  int supported = 0;  // cooperative launch available
+  int smem_max = 0;   // dynamic shared memory per CTA (opt-in limit less the static part)
+};
+
+const CoopLimits& coop_limits(int device) {
+  static CoopLimits lim[128];
+  static std::once_flag once[128];
+  SI_REQUIRE(device >= 0 && device < 128, SI_INVALID_ARGUMENT, "dense_evd: device ordinal");
+  std::call_once(once[device], [device] {
+    int coop = 0, smem = 0;
+    SI_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    SI_CUDA(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa{};
+    SI_CUDA(cudaFuncGetAttributes(&fa, k_tridiag_coop));
+    const int dyn = smem - static_cast<int>(fa.sharedSizeBytes);
+    SI_CUDA(cudaFuncSetAttribute(k_tridiag_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    lim[device].smem_max = dyn;
+    lim[device].supported = coop;
+  });
+  return lim[device];
+}
+
+// Dynamic shared memory available to k_backtransform_smem (set once per device).
+int bt_smem_max(int device) {
+  static int lim[128];
+  static std::once_flag once[128];
+  SI_REQUIRE(device >= 0 && device < 128, SI_INVALID_ARGUMENT, "dense_evd: device ordinal");
+  std::call_once(once[device], [device] {
+    int smem = 0;
+    SI_CUDA(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa{};
+    SI_CUDA(cudaFuncGetAttributes(&fa, k_backtransform_smem));
+    const int dyn = smem - static_cast<int>(fa.sharedSizeBytes);
+    SI_CUDA(cudaFuncSetAttribute(k_backtransform_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    lim[device] = dyn;
+  });
+  return lim[device];
+}
+
+// SPECTRAL_INIT_TRIDIAG=steps selects the multi-launch steps for every n
+// (read on every call, so one process can exercise both paths).
+bool coop_disabled() {
+  const char* v = std::getenv("SPECTRAL_INIT_TRIDIAG");
+  return v != nullptr && std::string(v) == "steps";
+}
+
+// Launch the single-launch tridiagonalisation if the matrix fits in the shared
+// memory of co-resident CTAs; false (nothing launched) otherwise.  About
+// 96 KB of rows per CTA: fewer CTAs make the barriers cheaper and leave SMs
+// to concurrent solves, the largest matrices use every SM.
+bool tridiag_coop(const Exec& ex, double* A, int n, double* d, double* e, double* tau, DevBuf<double>& work,
+                  DevBuf<unsigned>& flags) {
+  if (n < kTriMultiMin || n > kTriCoopMax || coop_disabled()) return false;
+  const CoopLimits& lim = coop_limits(ex.device);
+  if (!lim.supported) return false;
+  const double bytes = 8.0 * n * n;
+  int G = static_cast<int>(std::ceil(bytes / (96.0 * 1024.0)));
+  G = std::max(G, ceil_div(n, CT_RMAX));
+  G = std::min({G, n, ex.sms});
+  const int R = ceil_div(n, G);
+  G = ceil_div(n, R);
+  const size_t smem = sizeof(double) * static_cast<size_t>(R) * n;
+  if (R > CT_RMAX || smem > static_cast<size_t>(lim.smem_max)) return false;
+  int occ = 0;
+  SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tridiag_coop, CT_THREADS, smem));
+  if (G > occ * ex.sms) return false;
+  work.alloc(4 * static_cast<size_t>(n) + 2 * static_cast<size_t>(G), ex.stream);
+  flags.alloc(3, ex.stream);
+  flags.zero();
+  CoopTri p{};
+  p.A = A;
+  p.n = n;
+  p.G = G;
+  p.R = R;
+  p.d = d;
+  p.e = e;
+  p.tau = tau;
+  p.vbuf = work.get();
+  p.wbuf = work.get() + 2 * n;
+  p.share = work.get() + 4 * n;
+  p.vready = flags.get();
+  p.arrive = flags.get() + 1;
+  p.err = reinterpret_cast<int*>(flags.get() + 2);
+  void* args[] = {&p};
+  SI_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_tridiag_coop), dim3(G), dim3(CT_THREADS), args,
+                                      smem, ex.stream));
+  SI_LAUNCH_CHECK();
+  return true;
+}
+
 }  // namespace
 
 void dense_evd_dev(const Exec& ex, const OpDev& op, int k, double* evals_host, double* evecs, int ld) {
@@ -455,13 +934,27 @@ void dense_evd_dev(const Exec& ex, const OpDev& op, int k, double* evals_host, d
   SI_REQUIRE(op.v64 != nullptr || op.nnz == 0, SI_INVALID_ARGUMENT, "dense_evd: f64 values required");
   DevBuf<double> A(static_cast<size_t>(n) * n, ex.stream), d(n, ex.stream), e(n, ex.stream), tau(n, ex.stream),
       ev(MAXM, ex.stream);
-  A.zero();
-  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, int64_t(ex.sms) * 8)));
-  k_densify<<<grid, 256, 0, ex.stream>>>(n, op.indptr, op.indices, op.v64, op.diag, A.get());
-  SI_LAUNCH_CHECK();
-  k_mirror_lower<<<static_cast<int>(std::min<int64_t>((n * n + 255) / 256, int64_t(ex.sms) * 16)), 256, 0,
-                   ex.stream>>>(n, A.get());
-  SI_LAUNCH_CHECK();
+  DevBuf<int> bstart(n + 1, ex.stream), cand_blk(static_cast<size_t>(n) * k, ex.stream), piv(n, ex.stream),
+      sel_blk(MAXM, ex.stream);
+  DevBuf<double> es(n, ex.stream), cand(static_cast<size_t>(n) * k, ex.stream), lu(5 * n, ex.stream),
+      xv(n, ex.stream), sel_val(MAXM, ex.stream);
+  TriWork w{bstart.get(), es.get(), cand.get(), cand_blk.get(), lu.get(), piv.get(), xv.get(), sel_blk.get(),
+            sel_val.get()};
+  const int ni = static_cast<int>(n);
+  auto finish = [&] {
+    SI_CUDA(cudaMemsetAsync(evecs, 0, sizeof(double) * n * ld, ex.stream));
+    k_tri_eig<<<1, DT, 0, ex.stream>>>(d.get(), e.get(), ni, k, w, ev.get(), evecs, ld);
+    SI_LAUNCH_CHECK();
+    const size_t bt_smem = sizeof(double) * static_cast<size_t>(n) * k;
+    if (n >= 3 && n <= int64_t(BT_THREADS) * BT_RPT && bt_smem <= static_cast<size_t>(bt_smem_max(ex.device))) {
+      k_backtransform_smem<<<1, BT_THREADS, bt_smem, ex.stream>>>(A.get(), tau.get(), ni, evecs, ld, k);
+    } else {
+      k_backtransform<<<1, DT, 0, ex.stream>>>(A.get(), tau.get(), ni, evecs, ld, k);
+    }
+    SI_LAUNCH_CHECK();
+    SI_CUDA(cudaMemcpyAsync(evals_host, ev.get(), sizeof(double) * k, cudaMemcpyDeviceToHost, ex.stream));
+  };
+  densify(ex, op, A.get());
   if (n < kTriMultiMin) {
     // small matrices: one CTA (launch latency would dominate the step kernels)
     const size_t smem = sizeof(double) * 2 * n;
@@ -470,39 +963,25 @@ void dense_evd_dev(const Exec& ex, const OpDev& op, int k, double* evals_host, d
       SI_CUDA(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 8192 * 8));
       attr_set[ex.device] = true;
     }
-    k_tridiag<<<1, DT, smem, ex.stream>>>(A.get(), static_cast<int>(n), d.get(), e.get(), tau.get());
+    k_tridiag<<<1, DT, smem, ex.stream>>>(A.get(), ni, d.get(), e.get(), tau.get());
     SI_LAUNCH_CHECK();
-  } else {
-    const int ni = static_cast<int>(n);
-    DevBuf<double> vbuf(n, ex.stream), wbuf(n, ex.stream), partial((n + 7) / 8, ex.stream);
-    DevBuf<unsigned> counter(1, ex.stream);
-    counter.zero();
-    for (int j = 0; j + 2 < ni; ++j) {
-      const int len = ni - j - 1;
-      k_tri_house<<<1, 256, 0, ex.stream>>>(A.get(), ni, j, d.get(), e.get(), tau.get(), vbuf.get());
-      SI_LAUNCH_CHECK();
-      k_tri_matvec<<<(len + 7) / 8, 256, 0, ex.stream>>>(A.get(), ni, j, tau.get(), vbuf.get(), wbuf.get(),
-                                                         partial.get(), counter.get());
-      SI_LAUNCH_CHECK();
-      k_tri_update<<<std::min(len, ex.sms * 8), 256, 0, ex.stream>>>(A.get(), ni, j, tau.get(), vbuf.get(),
-                                                                    wbuf.get());
-      SI_LAUNCH_CHECK();
-    }
-    k_tri_last<<<1, 32, 0, ex.stream>>>(A.get(), ni, d.get(), e.get(), tau.get());
-    SI_LAUNCH_CHECK();
+    finish();
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
+    return;
   }
-  DevBuf<int> bstart(n + 1, ex.stream), cand_blk(static_cast<size_t>(n) * k, ex.stream), piv(n, ex.stream),
-      sel_blk(MAXM, ex.stream);
-  DevBuf<double> es(n, ex.stream), cand(static_cast<size_t>(n) * k, ex.stream), lu(5 * n, ex.stream),
-      xv(n, ex.stream), sel_val(MAXM, ex.stream);
-  TriWork w{bstart.get(), es.get(), cand.get(), cand_blk.get(), lu.get(), piv.get(), xv.get(), sel_blk.get(),
-            sel_val.get()};
-  SI_CUDA(cudaMemsetAsync(evecs, 0, sizeof(double) * n * ld, ex.stream));
-  k_tri_eig<<<1, DT, 0, ex.stream>>>(d.get(), e.get(), static_cast<int>(n), k, w, ev.get(), evecs, ld);
-  SI_LAUNCH_CHECK();
-  k_backtransform<<<1, DT, 0, ex.stream>>>(A.get(), tau.get(), static_cast<int>(n), evecs, ld, k);
-  SI_LAUNCH_CHECK();
-  SI_CUDA(cudaMemcpyAsync(evals_host, ev.get(), sizeof(double) * k, cudaMemcpyDeviceToHost, ex.stream));
+  DevBuf<double> cwork;
+  DevBuf<unsigned> cflags;
+  if (tridiag_coop(ex, A.get(), ni, d.get(), e.get(), tau.get(), cwork, cflags)) {
+    finish();
+    int err = 0;
+    SI_CUDA(cudaMemcpyAsync(&err, cflags.get() + 2, sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
+    if (err == 0) return;
+    // a wait of the single-launch kernel ran out: redo with the multi-launch steps
+    densify(ex, op, A.get());
+  }
+  tridiag_steps(ex, A.get(), ni, d.get(), e.get(), tau.get());
+  finish();
   SI_CUDA(cudaStreamSynchronize(ex.stream));
 }
 

@@ -116,20 +116,45 @@ __device__ double cta_sum(double v, double* red) {
 // Parallel cyclic Jacobi with one update phase per round: the round's
 // disjoint rotations J are applied as A' = J^T A J and V' = V J in a single
 // pass into second buffers (every element of A' depends on a 2 x 2 block of
-// A), so a round is two barriers.  The rotation angle uses one square root,
-// one division and one reciprocal square root:
+// A), so a round is two barriers.  The rotation angle is taken in single
+// precision,
 //   t = h sgn(d) / (|d| + sqrt(d^2 + h^2)),  d = a_qq - a_pp, h = 2 a_pq,
-//   c = 1/sqrt(1 + t^2), s = t c     (the smaller root of t^2 + 2 (d/h) t - 1).
-// On return A (diagonal) and V hold the result.
+//   c = 1/sqrt(1 + t^2), s = t c     (the smaller root of t^2 + 2 (d/h) t - 1),
+// and (c, s) are then normalised in double precision by two Newton steps
+// (c, s) *= 1.5 - (c^2 + s^2)/2, so every rotation is orthogonal to rounding:
+// A and V stay exactly similar / orthogonal, and an angle off by ~1e-7 only
+// leaves ~1e-7 of a_pq for the next sweep (quadratic convergence down to that
+// level, then a factor ~1e-7 per sweep).  No f64 square root or division on
+// the round's critical path.  On return A (diagonal) and V hold the result.
 __device__ void cta_jacobi_db(double* A, double* V, double* A2, double* V2, int s, int ld, double* red) {
   __shared__ double al[3 * MAXM + 2], be[3 * MAXM + 2];
-  __shared__ int pq[3 * MAXM + 2], rot[3 * MAXM + 2];
+  __shared__ int pq[3 * MAXM + 2];
+  constexpr int kItems = 4;  // per-thread update items resolved once when 2 s^2 <= 4 * threads
   const int s2 = s + (s & 1);
   const int np = s2 / 2;
+  const int nitems = 2 * s * s;
+  const bool pre = nitems <= kItems * static_cast<int>(blockDim.x);
+  int it_i[kItems], it_j[kItems];
+#pragma unroll
+  for (int q = 0; q < kItems; ++q) {
+    const int t = threadIdx.x + q * blockDim.x;
+    const int u = t < s * s ? t : t - s * s;
+    it_i[q] = u / s;
+    it_j[q] = u - (u / s) * s;
+  }
   double* cur = A;
   double* nxt = A2;
   double* vc = V;
   double* vn = V2;
+  auto update_item = [&](int t, int i, int j) {
+    if (t < s * s) {
+      const int qi = pq[i], qj = pq[j];
+      nxt[i * ld + j] = al[i] * (al[j] * cur[i * ld + j] + be[j] * cur[i * ld + qj]) +
+                        be[i] * (al[j] * cur[qi * ld + j] + be[j] * cur[qi * ld + qj]);
+    } else {
+      vn[i * ld + j] = al[j] * vc[i * ld + j] + be[j] * vc[i * ld + pq[j]];
+    }
+  };
   for (int sweep = 0; sweep < 40; ++sweep) {
     double off = 0.0, dia = 0.0;
     for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
@@ -156,48 +181,45 @@ __device__ void cta_jacobi_db(double* A, double* V, double* A2, double* V2, int 
           b = t;
         }
         double c = 1.0, sn = 0.0;
-        bool rotate = false;
         if (b < s) {
           const double apq = cur[a * ld + b];
           const double app = cur[a * ld + a], aqq = cur[b * ld + b];
           const double tiny = DBL_EPSILON * 1e-3;
           if (fabs(apq) > 1e-300 && apq * apq > tiny * tiny * fabs(app * aqq)) {
-            const double d = aqq - app, h = 2.0 * apq;
-            const double t = (d >= 0.0 ? h : -h) / (fabs(d) + sqrt(fma(d, d, h * h)));
-            c = rsqrt(fma(t, t, 1.0));
-            sn = t * c;
-            rotate = true;
+            const float d = static_cast<float>(aqq - app), h = static_cast<float>(2.0 * apq);
+            const float tf = (d >= 0.0f ? h : -h) / (fabsf(d) + sqrtf(fmaf(d, d, h * h)));
+            const float cf = rsqrtf(fmaf(tf, tf, 1.0f));
+            c = static_cast<double>(cf);
+            sn = static_cast<double>(tf) * static_cast<double>(cf);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+              const double f = fma(-0.5, fma(c, c, sn * sn), 1.5);
+              c *= f;
+              sn *= f;
+            }
           }
         }
         // new row/column a = c a - s b ; new b = s a + c b
         al[a] = c;
         be[a] = -sn;
         pq[a] = (b < s) ? b : a;
-        rot[a] = rotate;
         if (b < s) {
           al[b] = c;
           be[b] = sn;
           pq[b] = a;
-          rot[b] = rotate;
         }
       }
       __syncthreads();
-      for (int t = threadIdx.x; t < 2 * s * s; t += blockDim.x) {
-        if (t < s * s) {
-          const int i = t / s, j = t - (t / s) * s;
-          const int qi = pq[i], qj = pq[j];
-          double v;
-          if (rot[i] && qi == j) {
-            v = 0.0;  // the annihilated pair: exact zero
-          } else {
-            v = al[i] * (al[j] * cur[i * ld + j] + be[j] * cur[i * ld + qj]) +
-                be[i] * (al[j] * cur[qi * ld + j] + be[j] * cur[qi * ld + qj]);
-          }
-          nxt[i * ld + j] = v;
-        } else {
-          const int u = t - s * s;
-          const int k = u / s, j = u - (u / s) * s;
-          vn[k * ld + j] = al[j] * vc[k * ld + j] + be[j] * vc[k * ld + pq[j]];
+      if (pre) {
+#pragma unroll
+        for (int q = 0; q < kItems; ++q) {
+          const int t = threadIdx.x + q * blockDim.x;
+          if (t < nitems) update_item(t, it_i[q], it_j[q]);
+        }
+      } else {
+        for (int t = threadIdx.x; t < nitems; t += blockDim.x) {
+          const int u = t < s * s ? t : t - s * s;
+          update_item(t, u / s, u - (u / s) * s);
         }
       }
       __syncthreads();

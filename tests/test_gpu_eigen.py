@@ -205,3 +205,71 @@ def test_shift_invert_level_matches_golden(gpu_ctx, dataset):
     assert got == 2
     assert np.all(np.abs(vals - ref[:3]) < 1e-6), (vals, ref[:3])
     assert O.max_eigenpair_residual(lap, vals, vecs) < 1e-6
+
+
+# ---- dense EVD: single-launch vs multi-launch tridiagonalisation --------------------------------
+@pytest.mark.parametrize("n", [192, 517, 1999])
+@pytest.mark.parametrize("path", ["coop", "steps"])
+def test_dense_evd_tridiag_paths(gpu_ctx, monkeypatch, n, path):
+    """Both tridiagonalisations (one cooperative launch with the matrix in the
+    CTAs' shared memory; three launches per column) against LAPACK on a
+    random weighted graph Laplacian and on a path graph with known spectrum."""
+    import spectral_init_b200 as si
+    if path == "steps":
+        monkeypatch.setenv("SPECTRAL_INIT_TRIDIAG", "steps")
+    rng = np.random.default_rng(n)
+    # random sparse graph: a ring (connected) plus random chords, normalised Laplacian
+    rows = np.r_[np.arange(n), rng.integers(0, n, 4 * n)]
+    cols = np.r_[(np.arange(n) + 1) % n, rng.integers(0, n, 4 * n)]
+    w = rng.uniform(0.1, 1.0, rows.size)
+    a = sp.coo_matrix((w, (rows, cols)), shape=(n, n)).tocsr()
+    a = a + a.T
+    a.setdiag(0.0)
+    a.eliminate_zeros()
+    dinv = 1.0 / np.sqrt(np.asarray(a.sum(axis=1)).ravel())
+    lap = (sp.identity(n) - sp.diags(dinv) @ a @ sp.diags(dinv)).tocsr()
+    k = 6
+    vals, vecs = si.dense_evd(lap, k, ctx=gpu_ctx)
+    want = np.linalg.eigvalsh(lap.toarray())[:k]
+    assert np.max(np.abs(vals - want)) < 1e-10
+    assert np.allclose(vecs.T @ vecs, np.eye(k), atol=1e-10)
+    for j in range(k):
+        assert resid(lap, vecs[:, j], vals[j]) < 1e-10
+    # path Laplacian: 2 - 2 cos(pi j / n)
+    p = sp.diags([-np.ones(n - 1), np.r_[1.0, 2 * np.ones(n - 2), 1.0], -np.ones(n - 1)], [-1, 0, 1]).tocsr()
+    vals, vecs = si.dense_evd(p, 4, ctx=gpu_ctx)
+    assert np.allclose(vals, 2 - 2 * np.cos(np.pi * np.arange(4) / n), atol=1e-11)
+    for j in range(4):
+        assert resid(p, vecs[:, j], vals[j]) < 1e-10
+
+
+# ---- LOBPCG with 8- and 16-column blocks (register-tiled Gram, four-column update) -------------
+@pytest.mark.parametrize("nc,block", [(5, 0), (5, 7), (8, 0), (8, 10), (12, 0)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_lobpcg_wide_blocks(gpu_ctx, nc, block, precision):
+    """LOBPCG whose blocks are padded to 8 or 16 columns (m = the padded width
+    by default, m < width with an explicit block size) against LAPACK."""
+    import spectral_init_b200 as si
+    n = 1800
+    rng = np.random.default_rng(nc * 100 + block)
+    rows = np.r_[np.arange(n), rng.integers(0, n, 3 * n)]
+    cols = np.r_[(np.arange(n) + 1) % n, rng.integers(0, n, 3 * n)]
+    a = sp.coo_matrix((rng.uniform(0.1, 1.0, rows.size), (rows, cols)), shape=(n, n)).tocsr()
+    a = a + a.T
+    a.setdiag(0.0)
+    a.eliminate_zeros()
+    deg = np.asarray(a.sum(axis=1)).ravel()
+    dinv = 1.0 / np.sqrt(deg)
+    lap = (sp.identity(n) - sp.diags(dinv) @ a @ sp.diags(dinv)).tocsr()
+    cfg = si.SpectralInitConfig(precision=si.Precision.MIXED if precision == "mixed" else si.Precision.FP64,
+                                block_size=block)
+    out = si.lobpcg_solve(lap, nc, 42, False, np.sqrt(deg), cfg, ctx=gpu_ctx)
+    assert out is not None
+    (vals, vecs), _ = out
+    k = nc + 1
+    want = np.linalg.eigvalsh(lap.toarray())[:k]
+    # residual 1e-5 bounds the eigenvalue error by ~1e-10 / gap
+    assert np.max(np.abs(vals - want)) < 1e-7
+    assert np.allclose(vecs.T @ vecs, np.eye(k), atol=1e-8)
+    for j in range(k):
+        assert resid(lap, vecs[:, j], vals[j]) < 1e-5
