@@ -165,15 +165,13 @@ template <class XT>
 __global__ void __launch_bounds__(G4_THREADS) k_gram4(const XT* __restrict__ X, const XT* __restrict__ R,
                                                const XT* __restrict__ P, const XT* __restrict__ AX,
                                                const XT* __restrict__ AR, const XT* __restrict__ AP, int64_t n,
-                                               double* partial, double* out, unsigned* counter,
-                                               const int* __restrict__ stop) {
+                                               double* __restrict__ partial, const int* __restrict__ stop) {
   if (stop != nullptr && *stop != 0) return;
   // stages of [G4_TR][24] rows; after the main loop the same memory holds the
   // per-warp reduction buffer red[G4_WARPS][288] (f64)
   extern __shared__ __align__(16) unsigned char gram4_raw[];
   XT (*tile)[G4_TR][24] = reinterpret_cast<XT (*)[G4_TR][24]>(gram4_raw);
   double (*red)[288] = reinterpret_cast<double (*)[288]>(gram4_raw);
-  __shared__ bool last;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ai = 3 * (lane >> 3);  // S column base
   const int bj = 3 * (lane & 7);   // T column base
@@ -237,48 +235,46 @@ __global__ void __launch_bounds__(G4_THREADS) k_gram4(const XT* __restrict__ X, 
 #pragma unroll
     for (int q = 0; q < 3; ++q) red[warp][(ai + p) * 24 + bj + q] = acc[p][q];
   __syncthreads();
-  const int G = gridDim.x;
+  // one partial per entry and CTA (CTA-major); k_gram4_reduce adds them
   for (int e = tid; e < 288; e += G4_THREADS) {
-    double s = 0.0;
+    double sum = 0.0;
 #pragma unroll
-    for (int w = 0; w < G4_WARPS; ++w) s += red[w][e];
-    partial[static_cast<int64_t>(e) * G + blockIdx.x] = s;
+    for (int w = 0; w < G4_WARPS; ++w) sum += red[w][e];
+    partial[static_cast<int64_t>(blockIdx.x) * 288 + e] = sum;
   }
-  __threadfence();
+}
+
+// Adds the per-CTA partials of k_gram4 in CTA order (warp w takes CTAs w,
+// w + 8, ..., then the warp sums in warp order) and writes both 12 x 12
+// matrices (upper triangles mirrored).
+__global__ void __launch_bounds__(256) k_gram4_reduce(const double* __restrict__ partial, int nparts,
+                                                      double* __restrict__ out, const int* __restrict__ stop) {
+  if (stop != nullptr && *stop != 0) return;
+  __shared__ double red[8][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int e = blockIdx.x * 32 + lane;
+  double sum = 0.0;
+  if (e < 288)
+    for (int c = warp; c < nparts; c += 8) sum += partial[static_cast<int64_t>(c) * 288 + e];
+  red[warp][lane] = sum;
   __syncthreads();
-  if (tid == 0) last = (atomicAdd(counter, 1u) == static_cast<unsigned>(G) - 1);
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // finishing CTA: four entries per warp pass so a lane keeps many loads in flight
-  for (int e0 = warp * 4; e0 < 288; e0 += 4 * G4_WARPS) {
-    double s[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int c = lane; c < G; c += 32) {
+  if (warp != 0 || e >= 288) return;
+  double v = 0.0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) s[q] += partial[static_cast<int64_t>(e0 + q) * G + c];
+  for (int w = 0; w < 8; ++w) v += red[w][lane];
+  const int i = e / 24, j = e % 24;
+  if (j < 12) {
+    if (i <= j) {
+      out[i * 12 + j] = v;
+      out[j * 12 + i] = v;
     }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const double v = warp_sum(s[q]);
-      const int e = e0 + q;
-      const int i = e / 24, j = e % 24;
-      if (lane == 0) {
-        if (j < 12) {
-          if (i <= j) {
-            out[i * 12 + j] = v;
-            out[j * 12 + i] = v;
-          }
-        } else {
-          const int jj = j - 12;
-          if (i <= jj) {
-            out[144 + i * 12 + jj] = v;
-            out[144 + jj * 12 + i] = v;
-          }
-        }
-      }
+  } else {
+    const int jj = j - 12;
+    if (i <= jj) {
+      out[144 + i * 12 + jj] = v;
+      out[144 + jj * 12 + i] = v;
     }
   }
-  if (tid == 0) *counter = 0u;
 }
 
 // ---------------------------------------------------------------------------
@@ -1208,12 +1204,13 @@ void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, 
       resident[ti][ex.device] = std::max(1, r);
     }
     const int64_t ntiles = (n + G4_TR - 1) / G4_TR;
-    // at most two CTAs per SM: the finishing CTA adds 288 partials per CTA
-    const int grid = static_cast<int>(std::max<int64_t>(
-        1, std::min<int64_t>(ntiles, int64_t(ex.sms) * std::min(2, resident[ti][ex.device].load()))));
+    const int grid = static_cast<int>(
+        std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ex.sms) * resident[ti][ex.device].load())));
     w.ensure(static_cast<size_t>(grid) * 288, ex.stream);
-    k_gram4<XT><<<grid, G4_THREADS, gram4_smem_bytes<XT>(), ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4], blk[5], n,
-                                                                  w.partial.get(), out, w.counter.get(), stop);
+    k_gram4<XT><<<grid, G4_THREADS, gram4_smem_bytes<XT>(), ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4],
+                                                                        blk[5], n, w.partial.get(), stop);
+    SI_LAUNCH_CHECK();
+    k_gram4_reduce<<<9, 256, 0, ex.stream>>>(w.partial.get(), grid, out, stop);
     SI_LAUNCH_CHECK();
     return;
   }

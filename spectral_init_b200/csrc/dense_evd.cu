@@ -19,6 +19,8 @@
 #include <cstdlib>
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "si_internal.h"
 
@@ -261,6 +263,7 @@ constexpr int CT_RMAX = 16;                                    // rows per CTA
 constexpr int CT_CMAX = 4;                                     // columns per thread
 constexpr int64_t kTriCoopMax = int64_t(CT_THREADS) * CT_CMAX;  // 2048
 constexpr uint64_t kCoopWaitNs = 2000000000ull;                // 2 s per wait
+constexpr int kFlagStride = 32;                                // unsigned words per 128-byte line
 
 struct CoopTri {
   double* A;  // n x n, exactly symmetric on entry; reflector of step j goes to row j
@@ -287,12 +290,17 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-// One thread: wait until *p >= target.  False when the wait ran past the limit
-// (the error word is set) or another CTA gave up first.
+__device__ __forceinline__ void red_release_add_u32(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// One thread: wait until *p >= target, polling with a short back-off.  False
+// when the wait ran past the limit (the error word is set) or another CTA gave
+// up first.
 __device__ bool coop_wait(const unsigned* p, unsigned target, int* err) {
   if (ld_acquire_u32(p) >= target) return true;
   const uint64_t t0 = coop_ns();
   while (ld_acquire_u32(p) < target) {
+    __nanosleep(32);
     if (*reinterpret_cast<volatile int*>(err) != 0) return false;
     if (coop_ns() - t0 > kCoopWaitNs) {
       atomicExch(err, 1);
@@ -306,7 +314,6 @@ __global__ void __launch_bounds__(CT_THREADS, 1) k_tridiag_coop(CoopTri p) {
   extern __shared__ double rows[];  // [R][n]
   __shared__ double red[CT_THREADS / 32][CT_RMAX];
   __shared__ double s_v[CT_RMAX], s_w[CT_RMAX];
-  __shared__ double s_scal, s_K;
   __shared__ int s_ok;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int n = p.n, G = p.G, R = p.R, b = blockIdx.x;
@@ -321,35 +328,32 @@ __global__ void __launch_bounds__(CT_THREADS, 1) k_tridiag_coop(CoopTri p) {
     double* vb = p.vbuf + par * n;
     double* wb = p.wbuf + par * n;
     double* sh = p.share + par * G;
-    // (1) reflector of row j
-    if (j % G == b) {
+    // (1) reflector of row j, formed by warp 0 of the CTA holding the row
+    if (j % G == b && warp == 0) {
       const double* rj = rows + (j / G) * n;
       double part = 0.0;
-      for (int i = j + 2 + tid; i < n; i += CT_THREADS) part = fma(rj[i], rj[i], part);
-      const double sigma = block_sum_all(part, &red[0][0]);
-      if (tid == 0) {
-        const double alpha = rj[j + 1];
-        double t = 0.0, beta = alpha, scal = 0.0;
-        if (sigma > 0.0) {
-          const double nrm = sqrt(alpha * alpha + sigma);
-          beta = alpha >= 0.0 ? -nrm : nrm;
-          t = (beta - alpha) / beta;
-          scal = 1.0 / (alpha - beta);
-        }
-        s_scal = scal;
+      for (int i = j + 2 + lane; i < n; i += 32) part = fma(rj[i], rj[i], part);
+      const double sigma = warp_sum(part);
+      const double alpha = rj[j + 1];
+      double t = 0.0, beta = alpha, scal = 0.0;
+      if (sigma > 0.0) {
+        const double nrm = sqrt(alpha * alpha + sigma);
+        beta = alpha >= 0.0 ? -nrm : nrm;
+        t = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      if (lane == 0) {
         p.d[j] = rj[j];
         p.e[j] = beta;
         p.tau[j] = t;
       }
-      __syncthreads();
-      const double scal = s_scal;
-      for (int i = j + 1 + tid; i < n; i += CT_THREADS) {
+      for (int i = j + 1 + lane; i < n; i += 32) {
         const double vi = (i == j + 1) ? 1.0 : rj[i] * scal;
         vb[i] = vi;
         if (i >= j + 2) p.A[static_cast<int64_t>(j) * n + i] = vi;
       }
-      __syncthreads();
-      if (tid == 0) {
+      __syncwarp();
+      if (lane == 0) {
         __threadfence();
         st_release_u32(p.vready, static_cast<unsigned>(j + 1));
       }
@@ -358,9 +362,12 @@ __global__ void __launch_bounds__(CT_THREADS, 1) k_tridiag_coop(CoopTri p) {
     __syncthreads();
     if (!s_ok) return;
     const double tau = __ldcg(p.tau + j);
-    // (2) w = tau A v on this CTA's rows r > j
     // slots below l0 hold finished rows (r <= j)
     const int l0 = j >= b ? (j - b) / G + 1 : 0;
+    const int my_r = tid * G + b;
+    const bool my_live = tid < R && my_r > j && my_r < n;
+    const double my_v = my_live ? __ldcg(vb + my_r) : 0.0;
+    // (2) w = tau A v on this CTA's rows r > j
     double vc[CT_CMAX], acc[CT_RMAX];
 #pragma unroll
     for (int l = 0; l < CT_RMAX; ++l) acc[l] = 0.0;
@@ -377,50 +384,51 @@ __global__ void __launch_bounds__(CT_THREADS, 1) k_tridiag_coop(CoopTri p) {
 #pragma unroll
     for (int l = 0; l < CT_RMAX; ++l) {
       if (l >= l0 && l < R) {
-        const double s = warp_sum(acc[l]);
-        if (lane == 0) red[warp][l] = s;
+        const double sum = warp_sum(acc[l]);
+        if (lane == 0) red[warp][l] = sum;
       }
     }
     __syncthreads();
-    if (tid < R) {
-      const int r = tid * G + b;
-      if (r > j && r < n) {
-        double s = 0.0;
-        for (int w = 0; w < CT_THREADS / 32; ++w) s += red[w][tid];
-        const double wr = tau * s;
-        wb[r] = wr;
+    // own rows (threads 0 .. R - 1, all in warp 0): w_r, and this CTA's share of w.v
+    if (warp == 0) {
+      double wr = 0.0;
+      if (my_live) {
+        double sum = 0.0;
+        for (int w = 0; w < CT_THREADS / 32; ++w) sum += red[w][tid];
+        wr = tau * sum;
+        wb[my_r] = wr;
+      }
+      if (tid < R) {
         s_w[tid] = wr;
-        s_v[tid] = __ldcg(vb + r);
-      } else {
-        s_w[tid] = 0.0;
-        s_v[tid] = 0.0;
+        s_v[tid] = my_v;
       }
-    }
-    __syncthreads();
-    if (tid == 0) {
-      double s = 0.0;
-      for (int l = 0; l < R; ++l) s = fma(s_w[l], s_v[l], s);
-      sh[b] = s;
-      __threadfence();
-      atomicAdd(p.arrive, 1u);
-      s_ok = coop_wait(p.arrive, static_cast<unsigned>(j + 1) * static_cast<unsigned>(G), p.err) ? 1 : 0;
+      const double share = warp_sum(wr * my_v);
+      __syncwarp();  // the lanes' w stores are ordered before lane 0's fence
+      if (lane == 0) {
+        sh[b] = share;
+        __threadfence();
+        red_release_add_u32(p.arrive, 1u);
+        s_ok = coop_wait(p.arrive, static_cast<unsigned>(j + 1) * static_cast<unsigned>(G), p.err) ? 1 : 0;
+      }
     }
     __syncthreads();
     if (!s_ok) return;
-    // (3) K, w' and the rank-2 update of this CTA's rows
-    if (warp == 0) {
-      double s = 0.0;
-      for (int c = lane; c < G; c += 32) s += __ldcg(sh + c);
-      s = warp_sum(s);
-      if (lane == 0) s_K = 0.5 * tau * s;
+    // (3) w of this thread's columns and, in every warp, K = tau (w.v) / 2
+    // from the CTAs' shares in CTA order (the same sum in every warp)
+    double wcol[CT_CMAX];
+#pragma unroll
+    for (int q = 0; q < CT_CMAX; ++q) {
+      const int c = j + 1 + tid + q * CT_THREADS;
+      wcol[q] = c < n ? __ldcg(wb + c) : 0.0;
     }
-    __syncthreads();
-    const double K = s_K;
+    double ksum = 0.0;
+    for (int c = lane; c < G; c += 32) ksum += __ldcg(sh + c);
+    const double K = 0.5 * tau * warp_sum(ksum);
 #pragma unroll
     for (int q = 0; q < CT_CMAX; ++q) {
       const int c = j + 1 + tid + q * CT_THREADS;
       if (c < n) {
-        const double wc = fma(-K, vc[q], __ldcg(wb + c));
+        const double wc = fma(-K, vc[q], wcol[q]);
 #pragma unroll
         for (int l = 0; l < CT_RMAX; ++l) {
           if (l >= l0 && l < R && l * G + b < n) {
@@ -445,14 +453,15 @@ __global__ void __launch_bounds__(CT_THREADS, 1) k_tridiag_coop(CoopTri p) {
   }
 }
 
-// number of eigenvalues of T[l..r] smaller than x (Sturm sequence)
-__device__ int sturm_count(const double* d, const double* e, int l, int r, double x, double pivmin) {
+// number of eigenvalues of T[l..r] smaller than x (Sturm sequence; e2 holds
+// the squared off-diagonals)
+__device__ int sturm_count(const double* d, const double* e2, int l, int r, double x, double pivmin) {
   int cnt = 0;
   double q = d[l] - x;
   if (fabs(q) < pivmin) q = -pivmin;
   if (q < 0.0) ++cnt;
   for (int i = l + 1; i <= r; ++i) {
-    q = d[i] - x - e[i - 1] * e[i - 1] / q;
+    q = d[i] - x - e2[i - 1] / q;
     if (fabs(q) < pivmin) q = -pivmin;
     if (q < 0.0) ++cnt;
   }
@@ -462,6 +471,7 @@ __device__ int sturm_count(const double* d, const double* e, int l, int r, doubl
 struct TriWork {
   int* bstart;      // [n + 1]
   double* es;       // [n] split off-diagonals
+  double* e2;       // [n] their squares
   double* cand;     // [n * k]
   int* cand_blk;    // [n * k]
   double* lu;       // [5 * n]
@@ -472,30 +482,58 @@ struct TriWork {
 };
 
 __global__ void __launch_bounds__(DT) k_tri_eig(const double* __restrict__ d, const double* __restrict__ e, int n,
-                                                int k, TriWork w, double* evals_out, double* Y, int ld) {
+                                                int k, TriWork w, double* evals_out, double* Y, int ld,
+                                                int use_smem) {
   __shared__ int s_nb;
   __shared__ double s_tnorm;
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    double tn = 0.0;
-    for (int i = 0; i < n; ++i) {
-      const double rs = fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
-      tn = fmax(tn, rs);
-    }
-    s_tnorm = tn;
-    int nb = 0;
-    w.bstart[nb++] = 0;
-    for (int i = 0; i + 1 < n; ++i) {
+  __shared__ double s_red[32];
+  extern __shared__ double te_sm[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // diagonal, split off-diagonals and their squares: in shared memory behind
+  // the inverse-iteration arrays when it fits
+  const double* dd = d;
+  double* es = w.es;
+  double* e2 = w.e2;
+  if (use_smem) {
+    double* dsm = te_sm + 6 * n;
+    for (int i = tid; i < n; i += blockDim.x) dsm[i] = d[i];
+    dd = dsm;
+    es = te_sm + 7 * n;
+    e2 = te_sm + 8 * n;
+  }
+  // |T| (row sums) and the splits where an off-diagonal is negligible
+  double part = 0.0;
+  for (int i = tid; i < n; i += blockDim.x) {
+    part = fmax(part, fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0));
+    if (i + 1 < n) {
       const double off = fabs(e[i]);
-      if (off <= DBL_EPSILON * (fabs(d[i]) + fabs(d[i + 1])) || off <= 1e-300) {
-        w.es[i] = 0.0;
-        w.bstart[nb++] = i + 1;
-      } else {
-        w.es[i] = e[i];
-      }
+      const bool split = off <= DBL_EPSILON * (fabs(d[i]) + fabs(d[i + 1])) || off <= 1e-300;
+      es[i] = split ? 0.0 : e[i];
+      e2[i] = split ? 0.0 : e[i] * e[i];
     }
-    w.bstart[nb] = n;
-    s_nb = nb;
+  }
+  part = warp_max(part);
+  if (lane == 0) s_red[warp] = part;
+  __syncthreads();
+  // block starts in order (one warp: ballot and prefix count per 32 entries)
+  if (warp == 0) {
+    double tn = 0.0;
+    for (int i = lane; i < static_cast<int>(blockDim.x >> 5); i += 32) tn = fmax(tn, s_red[i]);
+    tn = warp_max(tn);
+    int cnt = 0;
+    for (int base = 0; base + 1 < n; base += 32) {
+      const int i = base + lane;
+      const bool f = i + 1 < n && es[i] == 0.0;
+      const unsigned bal = __ballot_sync(0xffffffffu, f);
+      if (f) w.bstart[1 + cnt + __popc(bal & ((1u << lane) - 1u))] = i + 1;
+      cnt += __popc(bal);
+    }
+    if (lane == 0) {
+      w.bstart[0] = 0;
+      w.bstart[cnt + 1] = n;
+      s_nb = cnt + 1;
+      s_tnorm = tn;
+    }
   }
   __syncthreads();
   const int nb = s_nb;
@@ -517,9 +555,9 @@ __global__ void __launch_bounds__(DT) k_tri_eig(const double* __restrict__ d, co
     lo = DBL_MAX;
     hi = -DBL_MAX;
     for (int i = l; i <= r; ++i) {
-      const double rad = (i > l ? fabs(w.es[i - 1]) : 0.0) + (i < r ? fabs(w.es[i]) : 0.0);
-      lo = fmin(lo, d[i] - rad);
-      hi = fmax(hi, d[i] + rad);
+      const double rad = (i > l ? fabs(es[i - 1]) : 0.0) + (i < r ? fabs(es[i]) : 0.0);
+      lo = fmin(lo, dd[i] - rad);
+      hi = fmax(hi, dd[i] + rad);
     }
     lo -= 2.0 * DBL_EPSILON * tnorm + pivmin;
     hi += 2.0 * DBL_EPSILON * tnorm + pivmin;
@@ -551,7 +589,7 @@ __global__ void __launch_bounds__(DT) k_tri_eig(const double* __restrict__ d, co
     for (int round = 0; round < 200; ++round) {
       if (item < nitems && s_live[item]) {
         const int b = item / k;
-        s_cnt[tid] = sturm_count(d, w.es, w.bstart[b], w.bstart[b + 1] - 1, point(s_lo[item], s_hi[item], pi), pivmin);
+        s_cnt[tid] = sturm_count(dd, e2, w.bstart[b], w.bstart[b + 1] - 1, point(s_lo[item], s_hi[item], pi), pivmin);
       }
       __syncthreads();
       int more = 0;
@@ -584,117 +622,147 @@ __global__ void __launch_bounds__(DT) k_tri_eig(const double* __restrict__ d, co
       const int l = w.bstart[b], r = w.bstart[b + 1] - 1;
       for (int it = 0; it < 200 && !converged(lo, hi); ++it) {
         const double mid = 0.5 * (lo + hi);
-        if (sturm_count(d, w.es, l, r, mid, pivmin) > t) hi = mid; else lo = mid;
+        if (sturm_count(dd, e2, l, r, mid, pivmin) > t) hi = mid; else lo = mid;
       }
       w.cand[q] = 0.5 * (lo + hi);
     }
   }
   __syncthreads();
-  if (tid != 0) return;
   // k smallest candidates (stable)
-  int nsel = 0;
-  for (int s = 0; s < k; ++s) {
-    int best = -1;
-    for (int q = 0; q < nb * k; ++q) {
-      if (w.cand[q] == DBL_MAX) continue;
-      bool taken = false;
-      for (int u = 0; u < nsel; ++u)
-        if (w.sel_blk[u] == q) taken = true;
-      if (taken) continue;
-      if (best < 0 || w.cand[q] < w.cand[best]) best = q;
+  __shared__ int s_nsel;
+  if (tid == 0) {
+    int nsel = 0;
+    for (int s = 0; s < k; ++s) {
+      int best = -1;
+      for (int q = 0; q < nb * k; ++q) {
+        if (w.cand[q] == DBL_MAX) continue;
+        bool taken = false;
+        for (int u = 0; u < nsel; ++u)
+          if (w.sel_blk[u] == q) taken = true;
+        if (taken) continue;
+        if (best < 0 || w.cand[q] < w.cand[best]) best = q;
+      }
+      if (best < 0) break;
+      w.sel_blk[nsel++] = best;
     }
-    if (best < 0) break;
-    w.sel_blk[nsel++] = best;
+    for (int s = 0; s < nsel; ++s) {
+      const int q = w.sel_blk[s];
+      evals_out[s] = w.cand[q];
+      w.sel_val[s] = w.cand[q];
+    }
+    s_nsel = nsel;
   }
-  for (int s = 0; s < nsel; ++s) {
-    const int q = w.sel_blk[s];
-    evals_out[s] = w.cand[q];
-    w.sel_val[s] = w.cand[q];
-  }
+  __syncthreads();
+  const int nsel = s_nsel;
+  // Eigenvectors by inverse iteration.  The LU factorisation and the two
+  // triangular sweeps are sequential (thread 0, working arrays in shared
+  // memory when they fit, reciprocals of the pivots formed in parallel);
+  // re-orthogonalisation and normalisation use the whole CTA.  Iteration stops
+  // after the second solve once the growth ||y|| shows a residual at rounding
+  // level (as LAPACK's dstein), at the latest after the fourth.
+  double* D = use_smem ? te_sm : w.lu;
+  double* DL = D + n;
+  double* DU = D + 2 * n;
+  double* DU2 = D + 3 * n;
+  double* RD = D + 4 * n;  // 1 / D
+  double* x = use_smem ? te_sm + 5 * n : w.xv;
+  int* piv = use_smem ? reinterpret_cast<int*>(te_sm + 9 * n) : w.piv;
+  double* red = s_red;
   const double tiny = DBL_EPSILON * fmax(tnorm, DBL_MIN);
-  double* D = w.lu;
-  double* DL = w.lu + n;
-  double* DU = w.lu + 2 * n;
-  double* DU2 = w.lu + 3 * n;
   for (int s = 0; s < nsel; ++s) {
     const int q = w.sel_blk[s];
     const int b = w.cand_blk[q];
     const int l = w.bstart[b], r = w.bstart[b + 1] - 1, sz = r - l + 1;
     const double lam = w.cand[q];
+    double bpart = 0.0;
+    for (int i = l + tid; i <= r; i += blockDim.x)
+      bpart = fmax(bpart, fabs(dd[i]) + (i > l ? fabs(es[i - 1]) : 0.0) + (i < r ? fabs(es[i]) : 0.0));
+    bpart = warp_max(bpart);
+    if ((tid & 31) == 0) red[tid >> 5] = bpart;
+    __syncthreads();
     double bnorm = 0.0;
-    for (int i = l; i <= r; ++i)
-      bnorm = fmax(bnorm, fabs(d[i]) + (i > l ? fabs(w.es[i - 1]) : 0.0) + (i < r ? fabs(w.es[i]) : 0.0));
-    // LU with partial pivoting of T_b - lam I
-    for (int i = 0; i < sz; ++i) {
-      D[i] = d[l + i] - lam;
-      DU[i] = (i + 1 < sz) ? w.es[l + i] : 0.0;
+    for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) bnorm = fmax(bnorm, red[i]);
+    // T_b - lam I, and the start vector
+    for (int i = tid; i < sz; i += blockDim.x) {
+      D[i] = dd[l + i] - lam;
+      DU[i] = (i + 1 < sz) ? es[l + i] : 0.0;
       DL[i] = DU[i];
       DU2[i] = 0.0;
-    }
-    for (int i = 0; i + 1 < sz; ++i) {
-      if (fabs(D[i]) >= fabs(DL[i])) {
-        if (D[i] == 0.0) D[i] = tiny;
-        const double f = DL[i] / D[i];
-        DL[i] = f;
-        D[i + 1] -= f * DU[i];
-        w.piv[i] = 0;
-      } else {
-        const double f = D[i] / DL[i];
-        D[i] = DL[i];
-        DL[i] = f;
-        const double tmp = DU[i];
-        DU[i] = D[i + 1];
-        D[i + 1] = tmp - f * D[i + 1];
-        if (i + 2 < sz) {
-          DU2[i] = DU[i + 1];
-          DU[i + 1] = -f * DU[i + 1];
-        }
-        w.piv[i] = 1;
-      }
-    }
-    for (int i = 0; i < sz; ++i)
-      if (fabs(D[i]) < tiny) D[i] = D[i] < 0.0 ? -tiny : tiny;
-    // start vector
-    for (int i = 0; i < sz; ++i) {
       double z0, z1;
       philox_normal2(0x0de75eedull + s, 7, static_cast<uint64_t>(i), z0, z1);
-      w.xv[i] = z0;
+      x[i] = z0;
     }
-    for (int it = 0; it < 4; ++it) {
-      // solve (T - lam I) y = x in place
-      double* x = w.xv;
+    __syncthreads();
+    // LU with partial pivoting
+    if (tid == 0) {
       for (int i = 0; i + 1 < sz; ++i) {
-        if (w.piv[i] == 0) {
-          x[i + 1] -= DL[i] * x[i];
+        if (fabs(D[i]) >= fabs(DL[i])) {
+          if (D[i] == 0.0) D[i] = tiny;
+          const double f = DL[i] / D[i];
+          DL[i] = f;
+          D[i + 1] -= f * DU[i];
+          piv[i] = 0;
         } else {
-          const double tmp = x[i];
-          x[i] = x[i + 1];
-          x[i + 1] = tmp - DL[i] * x[i];
+          const double f = D[i] / DL[i];
+          D[i] = DL[i];
+          DL[i] = f;
+          const double tmp = DU[i];
+          DU[i] = D[i + 1];
+          D[i + 1] = tmp - f * D[i + 1];
+          if (i + 2 < sz) {
+            DU2[i] = DU[i + 1];
+            DU[i + 1] = -f * DU[i + 1];
+          }
+          piv[i] = 1;
         }
       }
-      x[sz - 1] /= D[sz - 1];
-      if (sz >= 2) x[sz - 2] = (x[sz - 2] - DU[sz - 2] * x[sz - 1]) / D[sz - 2];
-      for (int i = sz - 3; i >= 0; --i) x[i] = (x[i] - DU[i] * x[i + 1] - DU2[i] * x[i + 2]) / D[i];
+    }
+    __syncthreads();
+    for (int i = tid; i < sz; i += blockDim.x) {
+      if (fabs(D[i]) < tiny) D[i] = D[i] < 0.0 ? -tiny : tiny;
+      RD[i] = 1.0 / D[i];
+    }
+    __syncthreads();
+    const double grow_ok = 1.0 / (static_cast<double>(sz) * DBL_EPSILON * fmax(bnorm, DBL_MIN));
+    for (int it = 0; it < 4; ++it) {
+      // solve (T - lam I) y = x in place
+      if (tid == 0) {
+        for (int i = 0; i + 1 < sz; ++i) {
+          if (piv[i] == 0) {
+            x[i + 1] -= DL[i] * x[i];
+          } else {
+            const double tmp = x[i];
+            x[i] = x[i + 1];
+            x[i + 1] = tmp - DL[i] * x[i];
+          }
+        }
+        x[sz - 1] *= RD[sz - 1];
+        if (sz >= 2) x[sz - 2] = (x[sz - 2] - DU[sz - 2] * x[sz - 1]) * RD[sz - 2];
+        for (int i = sz - 3; i >= 0; --i) x[i] = (x[i] - DU[i] * x[i + 1] - DU2[i] * x[i + 2]) * RD[i];
+      }
+      __syncthreads();
       // re-orthogonalise against earlier vectors of the same block in the cluster
       for (int u = 0; u < s; ++u) {
         const int qu = w.sel_blk[u];
         if (w.cand_blk[qu] != b) continue;
         if (fabs(w.sel_val[u] - lam) > 1e-3 * bnorm) continue;
-        double dot = 0.0;
-        for (int i = 0; i < sz; ++i) dot += Y[static_cast<int64_t>(l + i) * ld + u] * x[i];
-        for (int i = 0; i < sz; ++i) x[i] -= dot * Y[static_cast<int64_t>(l + i) * ld + u];
+        double part = 0.0;
+        for (int i = tid; i < sz; i += blockDim.x) part += Y[static_cast<int64_t>(l + i) * ld + u] * x[i];
+        const double dot = block_sum_all(part, red);
+        for (int i = tid; i < sz; i += blockDim.x) x[i] -= dot * Y[static_cast<int64_t>(l + i) * ld + u];
+        __syncthreads();
       }
-      double nrm = 0.0;
-      for (int i = 0; i < sz; ++i) nrm += x[i] * x[i];
-      nrm = sqrt(nrm);
-      if (!(nrm > 0.0)) {
-        for (int i = 0; i < sz; ++i) x[i] = (i == s % sz) ? 1.0 : 0.0;
-        nrm = 1.0;
-      }
-      for (int i = 0; i < sz; ++i) x[i] /= nrm;
+      double part = 0.0;
+      for (int i = tid; i < sz; i += blockDim.x) part += x[i] * x[i];
+      double nrm = sqrt(block_sum_all(part, red));
+      const bool degenerate = !(nrm > 0.0);
+      const double inv = degenerate ? 1.0 : 1.0 / nrm;
+      for (int i = tid; i < sz; i += blockDim.x) x[i] = degenerate ? ((i == s % sz) ? 1.0 : 0.0) : x[i] * inv;
+      __syncthreads();
+      if (it >= 1 && nrm >= grow_ok) break;  // uniform: nrm is the same in every thread
     }
-    for (int i = 0; i < n; ++i) Y[static_cast<int64_t>(i) * ld + s] = 0.0;
-    for (int i = 0; i < sz; ++i) Y[static_cast<int64_t>(l + i) * ld + s] = w.xv[i];
+    for (int i = tid; i < sz; i += blockDim.x) Y[static_cast<int64_t>(l + i) * ld + s] = x[i];
+    __syncthreads();
   }
 }
 
@@ -800,6 +868,91 @@ __global__ void __launch_bounds__(BT_THREADS) k_backtransform_smem(const double*
   for (int idx = tid; idx < n * k; idx += BT_THREADS) Y[static_cast<int64_t>(idx / k) * ld + idx % k] = ys[idx];
 }
 
+// The same product, blocked: reflectors are applied eight at a time from the
+// last block down, each block as one compact-WY product (the forward,
+// column-wise form of LAPACK's dlarft):
+//   H_j0 H_j0+1 ... H_j0+7 = I - V T V^T,   T upper triangular,
+//   T[i][i] = tau_i,  T[0:i, i] = -tau_i T[0:i, 0:i] (V^T V)[0:i, i],
+// so a block costs one pass of dot products (V^T V and V^T Y, one warp per
+// product, lanes over rows), a small triangular product and one pass
+// Y -= V (T V^T Y).  Y (n x k) and the block's reflectors stay in shared
+// memory; a reflector with tau = 0 gets a zero row and column of T.
+constexpr int BW_NB = 8;
+constexpr int BW_THREADS = 512;
+
+__global__ void __launch_bounds__(BW_THREADS) k_backtransform_wy(const double* __restrict__ A,
+                                                                 const double* __restrict__ tau, int n,
+                                                                 double* __restrict__ Y, int ld, int k) {
+  extern __shared__ double bw_sm[];
+  double* ys = bw_sm;          // [n][k]
+  double* U = bw_sm + n * k;   // [BW_NB][n]
+  __shared__ double G[BW_NB][BW_NB], T[BW_NB][BW_NB], Wt[BW_NB][MAXM], Wp[BW_NB][MAXM], st[BW_NB];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = BW_THREADS / 32;
+  for (int idx = tid; idx < n * k; idx += BW_THREADS) ys[idx] = Y[static_cast<int64_t>(idx / k) * ld + idx % k];
+  const int nref = n - 2;  // reflectors 0 .. n - 3
+  for (int bi = (nref + BW_NB - 1) / BW_NB - 1; bi >= 0; --bi) {
+    const int j0 = bi * BW_NB, nb = min(BW_NB, nref - j0);
+    const int r0 = j0 + 1, len = n - r0;  // rows where the block's reflectors can be nonzero
+    for (int idx = tid; idx < nb * len; idx += BW_THREADS) {
+      const int i = idx / len, r = r0 + idx % len;
+      const int j = j0 + i;
+      U[i * n + r] = r == j + 1 ? 1.0 : (r > j + 1 ? A[static_cast<int64_t>(j) * n + r] : 0.0);
+    }
+    if (tid < nb) st[tid] = tau[j0 + tid];
+    __syncthreads();
+    const int ng = nb * (nb + 1) / 2, nd = ng + nb * k;
+    for (int dd = warp; dd < nd; dd += NW) {
+      double acc = 0.0;
+      int a = 0, b = 0, v = 0;
+      if (dd < ng) {
+        int e = dd;
+        while (e >= nb - a) {
+          e -= nb - a;
+          ++a;
+        }
+        b = a + e;
+        for (int r = r0 + lane; r < n; r += 32) acc = fma(U[a * n + r], U[b * n + r], acc);
+      } else {
+        a = (dd - ng) / k;
+        v = (dd - ng) % k;
+        for (int r = r0 + lane; r < n; r += 32) acc = fma(U[a * n + r], ys[r * k + v], acc);
+      }
+      acc = warp_sum(acc);
+      if (lane == 0) {
+        if (dd < ng) G[a][b] = acc;
+        else Wt[a][v] = acc;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int i = 0; i < nb; ++i) {
+        T[i][i] = st[i];
+        for (int p = 0; p < i; ++p) {
+          double sum = 0.0;
+          for (int q = p; q < i; ++q) sum = fma(T[p][q], G[q][i], sum);
+          T[p][i] = -st[i] * sum;
+        }
+      }
+      for (int a = 0; a < nb; ++a)
+        for (int v = 0; v < k; ++v) {
+          double sum = 0.0;
+          for (int b = a; b < nb; ++b) sum = fma(T[a][b], Wt[b][v], sum);
+          Wp[a][v] = sum;
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < len * k; idx += BW_THREADS) {
+      const int r = r0 + idx / k, v = idx % k;
+      double sum = 0.0;
+      for (int a = 0; a < nb; ++a) sum = fma(U[a * n + r], Wp[a][v], sum);
+      ys[r * k + v] -= sum;
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < n * k; idx += BW_THREADS) Y[static_cast<int64_t>(idx / k) * ld + idx % k] = ys[idx];
+}
+
 }  // namespace
 
 namespace {
@@ -858,21 +1011,26 @@ const CoopLimits& coop_limits(int device) {
   return lim[device];
 }
 
-// Dynamic shared memory available to k_backtransform_smem (set once per device).
-int bt_smem_max(int device) {
-  static int lim[128];
-  static std::once_flag once[128];
+// Dynamic shared memory a kernel of this file may use on a device (the
+// opt-in limit less its static shared memory), with the attribute raised to
+// it on first use.
+template <class F>
+int smem_limit(int device, F* kernel) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<int, const void*>, int>> known;
   SI_REQUIRE(device >= 0 && device < 128, SI_INVALID_ARGUMENT, "dense_evd: device ordinal");
-  std::call_once(once[device], [device] {
-    int smem = 0;
-    SI_CUDA(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-    cudaFuncAttributes fa{};
-    SI_CUDA(cudaFuncGetAttributes(&fa, k_backtransform_smem));
-    const int dyn = smem - static_cast<int>(fa.sharedSizeBytes);
-    SI_CUDA(cudaFuncSetAttribute(k_backtransform_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
-    lim[device] = dyn;
-  });
-  return lim[device];
+  const void* key = reinterpret_cast<const void*>(kernel);
+  std::lock_guard<std::mutex> lk(mu);
+  for (const auto& kv : known)
+    if (kv.first.first == device && kv.first.second == key) return kv.second;
+  int smem = 0;
+  SI_CUDA(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  cudaFuncAttributes fa{};
+  SI_CUDA(cudaFuncGetAttributes(&fa, kernel));
+  const int dyn = smem - static_cast<int>(fa.sharedSizeBytes);
+  SI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+  known.push_back({{device, key}, dyn});
+  return dyn;
 }
 
 // SPECTRAL_INIT_TRIDIAG=steps selects the multi-launch steps for every n
@@ -903,7 +1061,8 @@ bool tridiag_coop(const Exec& ex, double* A, int n, double* d, double* e, double
   SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tridiag_coop, CT_THREADS, smem));
   if (G > occ * ex.sms) return false;
   work.alloc(4 * static_cast<size_t>(n) + 2 * static_cast<size_t>(G), ex.stream);
-  flags.alloc(3, ex.stream);
+  // the step flag, the barrier counter and the error word on separate 128-byte lines
+  flags.alloc(3 * kFlagStride, ex.stream);
   flags.zero();
   CoopTri p{};
   p.A = A;
@@ -917,8 +1076,8 @@ bool tridiag_coop(const Exec& ex, double* A, int n, double* d, double* e, double
   p.wbuf = work.get() + 2 * n;
   p.share = work.get() + 4 * n;
   p.vready = flags.get();
-  p.arrive = flags.get() + 1;
-  p.err = reinterpret_cast<int*>(flags.get() + 2);
+  p.arrive = flags.get() + kFlagStride;
+  p.err = reinterpret_cast<int*>(flags.get() + 2 * kFlagStride);
   void* args[] = {&p};
   SI_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_tridiag_coop), dim3(G), dim3(CT_THREADS), args,
                                       smem, ex.stream));
@@ -936,17 +1095,24 @@ void dense_evd_dev(const Exec& ex, const OpDev& op, int k, double* evals_host, d
       ev(MAXM, ex.stream);
   DevBuf<int> bstart(n + 1, ex.stream), cand_blk(static_cast<size_t>(n) * k, ex.stream), piv(n, ex.stream),
       sel_blk(MAXM, ex.stream);
-  DevBuf<double> es(n, ex.stream), cand(static_cast<size_t>(n) * k, ex.stream), lu(5 * n, ex.stream),
-      xv(n, ex.stream), sel_val(MAXM, ex.stream);
-  TriWork w{bstart.get(), es.get(), cand.get(), cand_blk.get(), lu.get(), piv.get(), xv.get(), sel_blk.get(),
+  DevBuf<double> es(n, ex.stream), e2(n, ex.stream), cand(static_cast<size_t>(n) * k, ex.stream),
+      lu(5 * n, ex.stream), xv(n, ex.stream), sel_val(MAXM, ex.stream);
+  TriWork w{bstart.get(), es.get(), e2.get(), cand.get(), cand_blk.get(), lu.get(), piv.get(), xv.get(), sel_blk.get(),
             sel_val.get()};
   const int ni = static_cast<int>(n);
   auto finish = [&] {
     SI_CUDA(cudaMemsetAsync(evecs, 0, sizeof(double) * n * ld, ex.stream));
-    k_tri_eig<<<1, DT, 0, ex.stream>>>(d.get(), e.get(), ni, k, w, ev.get(), evecs, ld);
+    const size_t te_smem = (sizeof(double) * 9 + sizeof(int)) * static_cast<size_t>(n);
+    const bool te_in_smem = te_smem <= static_cast<size_t>(smem_limit(ex.device, k_tri_eig));
+    k_tri_eig<<<1, DT, te_in_smem ? te_smem : 0, ex.stream>>>(d.get(), e.get(), ni, k, w, ev.get(), evecs, ld,
+                                                              te_in_smem ? 1 : 0);
     SI_LAUNCH_CHECK();
+    const size_t wy_smem = sizeof(double) * static_cast<size_t>(n) * (k + BW_NB);
     const size_t bt_smem = sizeof(double) * static_cast<size_t>(n) * k;
-    if (n >= 3 && n <= int64_t(BT_THREADS) * BT_RPT && bt_smem <= static_cast<size_t>(bt_smem_max(ex.device))) {
+    if (n >= 3 && wy_smem <= static_cast<size_t>(smem_limit(ex.device, k_backtransform_wy))) {
+      k_backtransform_wy<<<1, BW_THREADS, wy_smem, ex.stream>>>(A.get(), tau.get(), ni, evecs, ld, k);
+    } else if (n >= 3 && n <= int64_t(BT_THREADS) * BT_RPT &&
+               bt_smem <= static_cast<size_t>(smem_limit(ex.device, k_backtransform_smem))) {
       k_backtransform_smem<<<1, BT_THREADS, bt_smem, ex.stream>>>(A.get(), tau.get(), ni, evecs, ld, k);
     } else {
       k_backtransform<<<1, DT, 0, ex.stream>>>(A.get(), tau.get(), ni, evecs, ld, k);
@@ -974,7 +1140,7 @@ void dense_evd_dev(const Exec& ex, const OpDev& op, int k, double* evals_host, d
   if (tridiag_coop(ex, A.get(), ni, d.get(), e.get(), tau.get(), cwork, cflags)) {
     finish();
     int err = 0;
-    SI_CUDA(cudaMemcpyAsync(&err, cflags.get() + 2, sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
+    SI_CUDA(cudaMemcpyAsync(&err, cflags.get() + 2 * kFlagStride, sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
     SI_CUDA(cudaStreamSynchronize(ex.stream));
     if (err == 0) return;
     // a wait of the single-launch kernel ran out: redo with the multi-launch steps

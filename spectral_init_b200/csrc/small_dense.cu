@@ -24,7 +24,8 @@
 namespace si {
 namespace {
 
-constexpr int ST = 128;  // threads of the small-step CTA
+constexpr int ST = 128;       // threads of the small-step CTA (blocks of up to 8 columns)
+constexpr int ST_WIDE = 512;  // threads of the small-step CTA for wider blocks
 
 struct SmallSmem {
   double* A;
@@ -129,7 +130,7 @@ __device__ double cta_sum(double v, double* red) {
 __device__ void cta_jacobi_db(double* A, double* V, double* A2, double* V2, int s, int ld, double* red) {
   __shared__ double al[3 * MAXM + 2], be[3 * MAXM + 2];
   __shared__ int pq[3 * MAXM + 2];
-  constexpr int kItems = 4;  // per-thread update items resolved once when 2 s^2 <= 4 * threads
+  constexpr int kItems = 9;  // per-thread update items resolved once when 2 s^2 <= 9 * threads
   const int s2 = s + (s & 1);
   const int np = s2 / 2;
   const int nitems = 2 * s * s;
@@ -495,7 +496,7 @@ __device__ bool cta_rr_general(const double* gb, const double* ga, int P, const 
 // `ctrl` points to the CTA's shared-memory copy of the control block.
 __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns, int mode,
                                 double* smem) {
-  __shared__ double red[ST / 32];
+  __shared__ double red[ST_WIDE / 32];
   __shared__ double rc[SMAX / 2 + 1], rs[SMAX / 2 + 1], dsc[3 * MAXM], theta[MAXM], rn[MAXM];
   __shared__ int ra[SMAX / 2 + 1], rb[SMAX / 2 + 1], order[3 * MAXM], idx[3 * MAXM];
   __shared__ int sflag, sdone, s_na, s_withp;
@@ -683,7 +684,8 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
 
 // The control block is staged in shared memory for the whole step (the step
 // is a long chain of small dependent updates) and written back at the end.
-__global__ void __launch_bounds__(ST) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
+template <int NT>
+__global__ void __launch_bounds__(NT) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
                                                    int mode) {
   extern __shared__ double smem[];
   __shared__ LobpcgCtrl sctrl;
@@ -743,11 +745,17 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
   const size_t smem = sizeof(double) * 5 * LDS * LDS;
   static std::atomic<bool> attr_set[128];
   if (ex.device >= 0 && ex.device < 128 && !attr_set[ex.device]) {
-    SI_CUDA(cudaFuncSetAttribute(k_small_step, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    SI_CUDA(cudaFuncSetAttribute(k_small_step<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    SI_CUDA(cudaFuncSetAttribute(k_small_step<ST_WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
     attr_set[ex.device] = true;
   }
-  (void)m;
-  k_small_step<<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  // the Rayleigh-Ritz problem has up to ns * m rows: wide blocks get more threads
+  if (ns * m > 24)
+    k_small_step<ST_WIDE><<<1, ST_WIDE, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  else
+    k_small_step<ST><<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
   SI_LAUNCH_CHECK();
 }
 
