@@ -245,9 +245,10 @@ __global__ void __launch_bounds__(G4_THREADS) k_gram4(const XT* __restrict__ X, 
 }
 
 // Adds the per-CTA partials of k_gram4 in CTA order (warp w takes CTAs w,
-// w + 8, ..., then the warp sums in warp order) and writes both 12 x 12
-// matrices (upper triangles mirrored).
-__global__ void __launch_bounds__(256) k_gram4_reduce(const double* __restrict__ partial, int nparts,
+// w + 8, ..., then the warp sums in warp order) and writes both
+// (4 ns_out) x (4 ns_out) matrices (upper triangles mirrored); ns_out = 1
+// keeps only the first block of S and of AS (the Gram of X and AX alone).
+__global__ void __launch_bounds__(256) k_gram4_reduce(const double* __restrict__ partial, int nparts, int ns_out,
                                                       double* __restrict__ out, const int* __restrict__ stop) {
   if (stop != nullptr && *stop != 0) return;
   __shared__ double red[8][32];
@@ -263,18 +264,11 @@ __global__ void __launch_bounds__(256) k_gram4_reduce(const double* __restrict__
 #pragma unroll
   for (int w = 0; w < 8; ++w) v += red[w][lane];
   const int i = e / 24, j = e % 24;
-  if (j < 12) {
-    if (i <= j) {
-      out[i * 12 + j] = v;
-      out[j * 12 + i] = v;
-    }
-  } else {
-    const int jj = j - 12;
-    if (i <= jj) {
-      out[144 + i * 12 + jj] = v;
-      out[144 + jj * 12 + i] = v;
-    }
-  }
+  const int h = j / 12, jj = j % 12;  // h = 0: S^T S, h = 1: S^T AS
+  const int P = 4 * ns_out;
+  if (i > jj || i >= P || jj >= P) return;
+  out[h * P * P + i * P + jj] = v;
+  out[h * P * P + jj * P + i] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -426,7 +420,8 @@ __global__ void __maxnreg__(128)
 // ..., then the eight warp sums are added in warp order.
 template <int LD>
 __global__ void __launch_bounds__(256) k_gram_ld_reduce(const double* __restrict__ partial, int nparts, int m,
-                                                        double* __restrict__ out, const int* __restrict__ stop) {
+                                                        int ns_out, double* __restrict__ out,
+                                                        const int* __restrict__ stop) {
   using C = GramLd<LD>;
   constexpr int TS = C::TS;
   if (stop != nullptr && *stop != 0) return;
@@ -449,8 +444,8 @@ __global__ void __launch_bounds__(256) k_gram_ld_reduce(const double* __restrict
   if (ti == tj && p > q) return;  // lower half of a diagonal tile
   const int i = ti * TS + p, j = tj * TS + q;  // entry (i, j) of the 3LD x 3LD product, i <= j
   const int ci = i % LD, cj = j % LD;
-  if (ci >= m || cj >= m) return;
-  const int P = 3 * m;
+  if (ci >= m || cj >= m || i / LD >= ns_out || j / LD >= ns_out) return;
+  const int P = ns_out * m;
   const int I = (i / LD) * m + ci, J = (j / LD) * m + cj;
   double* o = out + h * P * P;
   o[I * P + J] = v;
@@ -1151,7 +1146,7 @@ int grid_rows(const Exec& ex, int64_t items, int threads = 256, int per_sm = 8) 
 }
 
 template <class XT, int LD>
-void gram_ld_launch(const Exec& ex, GramWork& w, const XT* const* blk, int m, int64_t n, double* out,
+void gram_ld_launch(const Exec& ex, GramWork& w, const XT* const* blk, int m, int ns_out, int64_t n, double* out,
                     const int* stop) {
   using C = GramLd<LD>;
   constexpr size_t smem = gram_ld_smem<XT, LD>();
@@ -1172,7 +1167,7 @@ void gram_ld_launch(const Exec& ex, GramWork& w, const XT* const* blk, int m, in
   k_gram_ld<XT, LD><<<grid, C::THREADS, smem, ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4], blk[5], n,
                                                            w.partial.get(), stop);
   SI_LAUNCH_CHECK();
-  k_gram_ld_reduce<LD><<<(C::ENTRIES + 31) / 32, 256, 0, ex.stream>>>(w.partial.get(), grid, m, out, stop);
+  k_gram_ld_reduce<LD><<<(C::ENTRIES + 31) / 32, 256, 0, ex.stream>>>(w.partial.get(), grid, m, ns_out, out, stop);
   SI_LAUNCH_CHECK();
 }
 
@@ -1182,16 +1177,23 @@ template <class XT>
 void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, int ns, int nblk, int m, int ld,
               int64_t n, double* out, const int* stop) {
   SI_REQUIRE(nblk >= 1 && nblk <= 8 && m >= 1 && nblk * m <= GMAXW, SI_INVALID_ARGUMENT, "gram: too many columns");
-  if (mode == GRAM_SYM2 && ns == 3 && nblk == 6 && m <= ld && (ld == 8 || ld == 16)) {
-    // the per-iteration LOBPCG Gram of 8- and 16-column blocks
+  // The per-iteration LOBPCG Gram ([X R P], [AX AR AP]) and the Gram of X and
+  // AX alone (start and final Rayleigh-Ritz) run on the register-tiled
+  // kernels; the latter passes X and AX three times and keeps the first block.
+  const bool iter = mode == GRAM_SYM2 && ns == 3 && nblk == 6;
+  const bool xonly = mode == GRAM_SYM2 && ns == 1 && nblk == 2;
+  const XT* const six[6] = {blk[0], xonly ? blk[0] : blk[1], xonly ? blk[0] : blk[2],
+                            xonly ? blk[1] : blk[3], xonly ? blk[1] : blk[4], xonly ? blk[1] : blk[5]};
+  const int ns_out = xonly ? 1 : 3;
+  if ((iter || xonly) && m <= ld && (ld == 8 || ld == 16)) {
     if (ld == 8)
-      gram_ld_launch<XT, 8>(ex, w, blk, m, n, out, stop);
+      gram_ld_launch<XT, 8>(ex, w, six, m, ns_out, n, out, stop);
     else
-      gram_ld_launch<XT, 16>(ex, w, blk, m, n, out, stop);
+      gram_ld_launch<XT, 16>(ex, w, six, m, ns_out, n, out, stop);
     return;
   }
-  if (mode == GRAM_SYM2 && ns == 3 && nblk == 6 && m == 4 && ld == 4) {
-    // the per-iteration LOBPCG Gram of 4-column blocks
+  if ((iter || xonly) && m == 4 && ld == 4) {
+    // 4-column blocks
     // resident CTAs per SM from the stage memory (set once per device)
     static std::atomic<int> resident[2][64];
     const int ti = sizeof(XT) == 8 ? 1 : 0;
@@ -1207,10 +1209,10 @@ void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, 
     const int grid = static_cast<int>(
         std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ex.sms) * resident[ti][ex.device].load())));
     w.ensure(static_cast<size_t>(grid) * 288, ex.stream);
-    k_gram4<XT><<<grid, G4_THREADS, gram4_smem_bytes<XT>(), ex.stream>>>(blk[0], blk[1], blk[2], blk[3], blk[4],
-                                                                        blk[5], n, w.partial.get(), stop);
+    k_gram4<XT><<<grid, G4_THREADS, gram4_smem_bytes<XT>(), ex.stream>>>(six[0], six[1], six[2], six[3], six[4],
+                                                                        six[5], n, w.partial.get(), stop);
     SI_LAUNCH_CHECK();
-    k_gram4_reduce<<<9, 256, 0, ex.stream>>>(w.partial.get(), grid, out, stop);
+    k_gram4_reduce<<<9, 256, 0, ex.stream>>>(w.partial.get(), grid, ns_out, out, stop);
     SI_LAUNCH_CHECK();
     return;
   }
