@@ -66,6 +66,8 @@ def parse_args():
     p.add_argument("--configs", action="store_true",
                    help="the parity configurations instead: the n=200k family graph (FP64 / mixed / learned) and "
                         "the n=1M graph with n_components=8 and the rSVD path; one JSON line each")
+    p.add_argument("--dense", action="store_true",
+                   help="the device dense eigensolver (level 0) at n = 300 / 1000 / 1900 instead, one JSON line")
     p.add_argument("--profile-solve", action="store_true",
                    help="one FP64 and one mixed eigensolve only (after one warm-up each), for ncu launch lists")
     return p.parse_args()
@@ -660,10 +662,53 @@ def run_configs(a):
     print(json.dumps(line), flush=True)
 
 
+def run_dense(a):
+    """One JSON line: the device dense eigensolver (level 0) on fuzzy-kNN graphs of a few sizes, device time
+    per solve with CUDA events on the library's stream."""
+    import torch
+    import spectral_init_b200 as si
+    from spectral_init_b200 import synthetic
+    from spectral_init_b200._lib import SiConfig, SiReport
+    from spectral_init_b200.warm_start import DeviceLaplacian
+    dev = torch.device("cuda", 0)
+    ctx = si.Context(0)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(lib.si_ctx_stream(ctx.ptr), device=dev)
+    out = {"config": "dense eigensolver (level 0), n_components=2: fuzzy-kNN graphs, 4-cluster Gaussian mixture "
+                     "in 20-D (unit centre spread), k=15, seed 7", "sizes": {}}
+    for n in (300, 1000, 1900):
+        ip, ix, dv = synthetic.fuzzy_knn_graph_gpu(n, 15, 4, 20, seed=7, center_std=1.0, device=dev)
+        lap = DeviceLaplacian((ip, ix, dv, n), ctx=ctx)
+        cfg = SiConfig()
+        lib.si_config_default(C.byref(cfg))
+        cfg.force_level = 0
+        vals = (C.c_double * 3)()
+        vecs = torch.empty(n, 3, dtype=torch.float64, device=dev)
+        lev = C.c_int32(-1)
+        rep = SiReport()
+        times = []
+        for _ in range(max(1, a.warmup) + max(1, a.steps)):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.check(lib.si_solve_eigenproblem(ctx.ptr, C.byref(lap.op()), 2, a.seed, lap.sqrt_deg.data_ptr(),
+                                                C.byref(cfg), vals, vecs.data_ptr(), C.byref(lev), C.byref(rep)))
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        times = times[max(1, a.warmup):]
+        out["sizes"][str(n)] = {"ms": statistics.mean(times), "level": lev.value, "eigenvalues": list(vals[:]),
+                                "max_residual": rep.max_residual}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     a = parse_args()
     if a.components and a.impl == "ours":
         run_components(a)
+        return
+    if a.dense and a.impl == "ours":
+        run_dense(a)
         return
     if a.configs and a.impl == "ours":
         run_configs(a)
