@@ -28,7 +28,8 @@ namespace si {
 namespace {
 
 constexpr int DT = 1024;
-constexpr int TE_MS_ITEMS = 32;  // multisection when at most this many (block, index) items
+constexpr int TE_MS_ITEMS = 32;   // multisection when at most this many (block, index) items
+constexpr int TE_MS_POINTS = 96;  // at most this many Sturm points per item and round
 constexpr int64_t kTriMultiMin = 192;  // from this n the tridiagonalisation runs as multi-CTA steps
 
 __global__ void k_densify(int64_t n, const uint64_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
@@ -574,7 +575,9 @@ __global__ void __launch_bounds__(DT) k_tri_eig(const double* __restrict__ d, co
     __shared__ double s_lo[TE_MS_ITEMS], s_hi[TE_MS_ITEMS];
     __shared__ int s_live[TE_MS_ITEMS];
     __shared__ int s_cnt[DT];
-    const int P = static_cast<int>(blockDim.x) / nitems;
+    // points per item: each Sturm count is a chain of n FP64 divisions, so past
+    // ~96 points per item the SM's FP64 pipe, not the chain, sets the round time
+    const int P = min(static_cast<int>(blockDim.x) / nitems, TE_MS_POINTS);
     if (tid < nitems) {
       double lo = 0.0, hi = 0.0;
       const bool ok = item_interval(tid, lo, hi);
