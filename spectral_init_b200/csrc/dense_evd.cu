@@ -244,16 +244,19 @@ __global__ void k_tri_last(const double* A, int n, double* d, double* e, double*
 // The same Householder steps with the matrix held in the shared memory of G
 // co-resident CTAs (cooperative launch): row r lives in CTA r % G, slot r / G,
 // so a step touches on-chip data plus two n-vectors in L2.  Step j:
-//   (1) the CTA holding row j forms the reflector from that row (A is kept
-//       exactly symmetric, so row j equals column j), writes v, d, e, tau and
-//       the reflector (row j of A in global memory) and publishes the step
-//       with a release store;
-//   (2) every CTA computes w_r = tau (A v)_r for its rows r > j and its share
-//       of w.v; grid barrier;
-//   (3) every CTA adds the shares in CTA order, K = tau (w.v) / 2,
-//       w' = w - K v, and updates its rows A -= v w'^T + w' v^T, each entry
-//       as round(v_r w'_c) + round(w'_r v_c) so entries (r, c) and (c, r)
-//       stay identical.
+//   (1) warp 0 of the CTA holding row j forms the reflector from that row
+//       (A is kept exactly symmetric, so row j equals column j), writes v, d,
+//       e, tau and the reflector (row j of A in global memory) and publishes
+//       the step with a release store (no CTA-wide barrier on this path);
+//   (2) every CTA computes w_r = tau (A v)_r for its rows r > j; warp 0 adds
+//       its share of w.v and arrives at the grid barrier (a release add on a
+//       counter on its own 128-byte line, pollers back off 32 ns);
+//   (3) every warp of every CTA adds the shares in CTA order (the same sum
+//       everywhere), K = tau (w.v) / 2, w' = w - K v, and the CTA updates its
+//       rows A -= v w'^T + w' v^T, each entry as round(v_r w'_c) +
+//       round(w'_r v_c) so entries (r, c) and (c, r) stay identical.
+// Four CTA barriers a step; own-row v and the columns of w are loaded ahead of
+// the reductions that need them.
 // v, w and the shares are double-buffered by step parity: a buffer is written
 // again two steps later, after a barrier that all of its readers have passed.
 // Every wait is bounded: a CTA that waits longer than the limit sets the error
