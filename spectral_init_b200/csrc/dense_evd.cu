@@ -7,12 +7,15 @@
 //      shared memory of co-resident CTAs up to 2048 rows, and three launches
 //      per column above that;
 //   3. split T where off-diagonals are negligible, then for every block the
-//      smallest eigenvalues by Sturm-count bisection; the k smallest overall
-//      are kept;
+//      smallest eigenvalues by Sturm-count multisection (bisection when there
+//      are many blocks) to LAPACK dstebz's default tolerance eps |T|; the k
+//      smallest overall are kept;
 //   4. eigenvectors of T by inverse iteration restricted to the block (LU with
 //      partial pivoting of T - lambda I), re-orthogonalised within clusters of
-//      close eigenvalues (modified Gram-Schmidt);
-//   5. back-transformation v = Q y with the stored reflectors.
+//      close eigenvalues (modified Gram-Schmidt), stopped as LAPACK's dstein
+//      once the growth shows a rounding-level residual;
+//   5. back-transformation v = Q y with the stored reflectors (compact-WY
+//      blocks of eight when Y and a block fit in shared memory).
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
