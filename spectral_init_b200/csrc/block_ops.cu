@@ -969,9 +969,11 @@ struct Vec16<float> {
 };
 
 // LOBPCG update for 8- and 16-column blocks: LD / 4 threads per row, each
-// producing four output columns from the whole input rows (16-byte loads; the
-// threads of a row share the sectors), coefficients from shared memory
-// (zero outside the m x m block).  Same formulas as k_lobpcg_update.
+// producing four output columns.  A thread loads only its own four input
+// columns of each block (so a warp's loads are contiguous) and takes the
+// row's other columns from the row's lanes by warp shuffles; coefficients come
+// from shared memory (zero outside the m x m block).  Same formulas as
+// k_lobpcg_update.
 template <class XT, int LD>
 __global__ void __launch_bounds__(256) k_lobpcg_update_q(LobpcgBlocks<XT> b, const LobpcgCtrl* __restrict__ ctrl,
                                                          int64_t n, int init_mode) {
@@ -1006,22 +1008,32 @@ __global__ void __launch_bounds__(256) k_lobpcg_update_q(LobpcgBlocks<XT> b, con
     if (done) continue;  // uniform
     double xn[4] = {0.0, 0.0, 0.0, 0.0}, axn[4] = {0.0, 0.0, 0.0, 0.0};
     double pn[4] = {0.0, 0.0, 0.0, 0.0}, apn[4] = {0.0, 0.0, 0.0, 0.0};
-    // out[jj] += sum_c in_a[c] C[c][j0 + jj], out2[jj] += sum_c in_b[c] C[c][j0 + jj]
+    // out[jj] += sum_c in_a[c] C[c][j0 + jj], out2[jj] += sum_c in_b[c] C[c][j0 + jj];
+    // column c of the row is held by lane (first lane of the row) + c / 4
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    const int row_lane0 = lane & ~(TPR - 1);
     auto accumulate = [&](const XT* ina, const XT* inb, int w, double* outa, double* outb) {
+      XT va[4], vb[4];
 #pragma unroll
-      for (int c0 = 0; c0 < LD; c0 += EPV) {
-        XT va[EPV], vb[EPV];
-        *reinterpret_cast<V*>(va) = *reinterpret_cast<const V*>(ina + o + c0);
-        *reinterpret_cast<V*>(vb) = *reinterpret_cast<const V*>(inb + o + c0);
+      for (int h = 0; h < 4; h += EPV) {
+        *reinterpret_cast<V*>(va + h) = *reinterpret_cast<const V*>(ina + o + j0 + h);
+        *reinterpret_cast<V*>(vb + h) = *reinterpret_cast<const V*>(inb + o + j0 + h);
+      }
+      double da[4], db[4];
 #pragma unroll
-        for (int cc = 0; cc < EPV; ++cc) {
-          const double a = static_cast<double>(va[cc]), bb = static_cast<double>(vb[cc]);
+      for (int h = 0; h < 4; ++h) {
+        da[h] = static_cast<double>(va[h]);
+        db[h] = static_cast<double>(vb[h]);
+      }
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj) {
-            const double cf = sC[w][c0 + cc][j0 + jj];
-            outa[jj] = fma(a, cf, outa[jj]);
-            outb[jj] = fma(bb, cf, outb[jj]);
-          }
+      for (int c = 0; c < LD; ++c) {
+        const double a = __shfl_sync(0xffffffffu, da[c % 4], row_lane0 + c / 4);
+        const double bb = __shfl_sync(0xffffffffu, db[c % 4], row_lane0 + c / 4);
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const double cf = sC[w][c][j0 + jj];
+          outa[jj] = fma(a, cf, outa[jj]);
+          outb[jj] = fma(bb, cf, outb[jj]);
         }
       }
     };
