@@ -667,14 +667,24 @@ def select_eigenvectors(vals: np.ndarray, vecs: np.ndarray, n_components: int) -
 
 
 def normalize_signs(coords: np.ndarray) -> None:
-    """Flip each column so its first largest-|.| element is positive."""
+    """Flip each column so its first largest-|.| element is positive
+    (src/scaling.rs:62-74).
+
+    The crate reduces with ``b.abs().total_cmp(&a.abs()).is_gt()``: on the
+    non-negative |x| (sign bit clear) total_cmp is the order of the bit
+    patterns as unsigned integers, so a NaN ranks above +inf (NaNs by payload)
+    and ties keep the earlier row.  ``signum`` is -1 for negatives and -0.0
+    and NaN for NaN, and only ``sign < 0`` flips, so a NaN maximum never flips.
+    """
     for c in range(coords.shape[1]):
-        col = coords[:, c]
+        col = np.ascontiguousarray(coords[:, c], dtype=np.float64)
         if col.size == 0:
             continue
-        i = int(np.argmax(np.abs(col)))  # first maximum, like the strict-> reduce
-        if np.sign(col[i]) < 0 or (col[i] == 0 and math.copysign(1.0, col[i]) < 0):
-            coords[:, c] = -col
+        keys = col.view(np.uint64) & np.uint64(0x7FFFFFFFFFFFFFFF)
+        i = int(np.argmax(keys))  # first maximum, like the strict-> reduce
+        v = float(col[i])
+        if not math.isnan(v) and math.copysign(1.0, v) < 0:
+            coords[:, c] = -coords[:, c]
 
 
 def scale_coords(coords: np.ndarray, max_coord: float) -> np.ndarray:

@@ -705,15 +705,19 @@ __global__ void k_gather_cols(const XI* in, int ld_in, XO* out, int ld_out, int6
 // per column: (max |x|, first index) ; deterministic
 __global__ void k_argmax_abs(const double* x, int64_t n, int k, int ld, double* pval, long long* pidx,
                              unsigned* counter, double* sign_out) {
-  __shared__ double sv[256];
+  // |x| is ranked by f64::total_cmp, as the crate's reduce does: the bit
+  // pattern of |x| (sign bit clear) compared as an integer, so a NaN ranks
+  // above +inf.  The partial keys travel through the f64 partial buffer
+  // bit for bit.
+  __shared__ long long sv[256];
   __shared__ long long si_[256];
   __shared__ bool last;
   for (int c = 0; c < k; ++c) {
-    double best = -1.0;
+    long long best = -1;
     long long bi = -1;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
-      const double a = fabs(x[i * ld + c]);
+      const long long a = __double_as_longlong(x[i * ld + c]) & 0x7fffffffffffffffLL;
       if (a > best) {
         best = a;
         bi = i;
@@ -724,9 +728,9 @@ __global__ void k_argmax_abs(const double* x, int64_t n, int k, int ld, double* 
     __syncthreads();
     for (int o = blockDim.x / 2; o > 0; o >>= 1) {
       if (threadIdx.x < o) {
-        const double a2 = sv[threadIdx.x + o];
+        const long long a2 = sv[threadIdx.x + o];
         const long long i2 = si_[threadIdx.x + o];
-        const double a1 = sv[threadIdx.x];
+        const long long a1 = sv[threadIdx.x];
         const long long i1 = si_[threadIdx.x];
         if (i2 >= 0 && (a2 > a1 || (a2 == a1 && (i1 < 0 || i2 < i1)))) {
           sv[threadIdx.x] = a2;
@@ -736,7 +740,7 @@ __global__ void k_argmax_abs(const double* x, int64_t n, int k, int ld, double* 
       __syncthreads();
     }
     if (threadIdx.x == 0) {
-      pval[static_cast<int64_t>(blockIdx.x) * SMAX + c] = sv[0];
+      pval[static_cast<int64_t>(blockIdx.x) * SMAX + c] = __longlong_as_double(sv[0]);
       pidx[static_cast<int64_t>(blockIdx.x) * SMAX + c] = si_[0];
     }
     __syncthreads();
@@ -749,18 +753,19 @@ __global__ void k_argmax_abs(const double* x, int64_t n, int k, int ld, double* 
   __threadfence();
   if (threadIdx.x < k) {
     const int c = threadIdx.x;
-    double best = -1.0;
+    long long best = -1;
     long long bi = -1;
     for (int b = 0; b < static_cast<int>(gridDim.x); ++b) {
-      const double a = pval[static_cast<int64_t>(b) * SMAX + c];
+      const long long a = __double_as_longlong(pval[static_cast<int64_t>(b) * SMAX + c]);
       const long long i = pidx[static_cast<int64_t>(b) * SMAX + c];
       if (i >= 0 && (a > best || (a == best && (bi < 0 || i < bi)))) {
         best = a;
         bi = i;
       }
     }
-    // Rust f64::signum: -1 for negative values and -0.0
-    sign_out[c] = (bi >= 0 && signbit(x[bi * ld + c])) ? -1.0 : 1.0;
+    // Rust f64::signum: -1 for negative values and -0.0; NaN (never flipped) for NaN
+    const double v = bi >= 0 ? x[bi * ld + c] : 1.0;
+    sign_out[c] = (!isnan(v) && signbit(v)) ? -1.0 : 1.0;
   }
   if (threadIdx.x == 0) *counter = 0u;
 }

@@ -17,7 +17,18 @@
 // serialised by the caller.  The first call on a device looks up the array's
 // device address (cudaGetSymbolAddress with that device current, which may
 // load the module there), so that call should come before any stream capture.
+// The address is cached per CUDA context, not per device ordinal: if the
+// device's primary context is destroyed and created again (cudaDeviceReset by
+// the host program or another library), the module is loaded anew, the array
+// moves, and the next call looks its address up again.
 // Limit: k <= 64 columns; any n.
+//
+// Column maximum as the crate ranks it: |x| compared with f64::total_cmp, so
+// a NaN (whose |.| has the sign bit clear) ranks above +inf, NaNs rank by
+// payload, and ties keep the first row; a column whose maximum is a NaN is
+// never flipped (signum(NaN) = NaN is not < 0).
+#include <cuda.h>
+
 #include <algorithm>
 #include <mutex>
 
@@ -35,7 +46,7 @@ constexpr int kNaMaxCtas = 512;
 // by every CTA before the last one reads them, and `sign` is written by that
 // CTA before the apply kernel reads it.
 struct SignScratch {
-  double val[kNaMaxCtas * kNoAllocMaxCols];
+  long long val[kNaMaxCtas * kNoAllocMaxCols];
   long long idx[kNaMaxCtas * kNoAllocMaxCols];
   double sign[kNoAllocMaxCols];
   unsigned ticket;
@@ -45,24 +56,70 @@ static __device__ __align__(256) unsigned char g_sign_scratch[sizeof(SignScratch
 
 constexpr int kMaxDevices = 64;
 std::mutex g_addr_mu;
-void* g_addr[kMaxDevices] = {};
+struct AddrEntry {
+  unsigned long long ctx_id = 0;  // context the address belongs to (0: none yet)
+  void* ptr = nullptr;
+};
+AddrEntry g_addr[kMaxDevices];
 
-// Device address of the scratch array on the current device (looked up once
-// per device; the array's host-side name is not a device address).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Identifier of the calling thread's current CUDA context (unique for the
+// life of the process; a re-created primary context gets a new one).
+unsigned long long current_context_id() {
+  static std::once_flag once;
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(p);
+  });
+  SI_REQUIRE(get_current != nullptr && get_id != nullptr, SI_CUDA_ERROR,
+             "normalize_signs_noalloc: cuCtxGetCurrent / cuCtxGetId are not available from the driver");
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  SI_REQUIRE(get_current(&c) == CUDA_SUCCESS && c != nullptr, SI_CUDA_ERROR,
+             "normalize_signs_noalloc: no current CUDA context");
+  SI_REQUIRE(get_id(c, &id) == CUDA_SUCCESS && id != 0, SI_CUDA_ERROR,
+             "normalize_signs_noalloc: cuCtxGetId failed");
+  return id;
+}
+
+// Device address of the scratch array in the current context of `device`
+// (the array's host-side name is not a device address).  Looked up once per
+// context: the first call on a device, and again after that device's context
+// was re-created.
 SignScratch* scratch_address(int device) {
   SI_REQUIRE(device >= 0 && device < kMaxDevices, SI_INVALID_ARGUMENT,
              "normalize_signs_noalloc: device ordinal beyond the supported 64 devices");
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lock(g_addr_mu);
-  if (g_addr[device] == nullptr) {
+  AddrEntry& e = g_addr[device];
+  if (e.ptr == nullptr || e.ctx_id != ctx) {
     void* p = nullptr;
     SI_CUDA(cudaGetSymbolAddress(&p, g_sign_scratch));
     SI_REQUIRE(p != nullptr, SI_CUDA_ERROR, "normalize_signs_noalloc: scratch symbol has no device address");
-    g_addr[device] = p;
+    e.ptr = p;
+    e.ctx_id = ctx;
   }
-  return static_cast<SignScratch*>(g_addr[device]);
+  return static_cast<SignScratch*>(e.ptr);
 }
 
-__device__ __forceinline__ bool better(double a2, long long i2, double a1, long long i1) {
+// Key of |x| whose unsigned order is f64::total_cmp on |x| (the sign bit of
+// |x| is clear, so NaNs sort above +inf by payload); -1 marks "no row".
+__device__ __forceinline__ long long abs_key(double v) {
+  return __double_as_longlong(v) & 0x7fffffffffffffffLL;
+}
+
+__device__ __forceinline__ bool better(long long a2, long long i2, long long a1, long long i1) {
   return i2 >= 0 && (a2 > a1 || (a2 == a1 && (i1 < 0 || i2 < i1)));
 }
 
@@ -72,22 +129,22 @@ __device__ __forceinline__ bool better(double a2, long long i2, double a1, long 
 // with R = 256 / k rows per CTA, so a warp reads consecutive elements.
 __global__ void __launch_bounds__(kNaThreads) k_argmax_abs_rows(const double* __restrict__ x, int64_t n, int k,
                                                                 SignScratch* __restrict__ s) {
-  __shared__ double sv[kNaThreads];
+  __shared__ long long sv[kNaThreads];
   __shared__ long long sx[kNaThreads];
   __shared__ bool last;
   const int t = threadIdx.x;
   const int R = kNaThreads / k;
   const int c = t % k;
   const int r = t / k;
-  double best = -1.0;
+  long long best = -1;
   long long bi = -1;
   if (r < R) {
     const int64_t step = static_cast<int64_t>(gridDim.x) * R;
     int64_t i = static_cast<int64_t>(blockIdx.x) * R + r;
     for (; i + 3 * step < n; i += 4 * step) {
-      double a[4];
+      long long a[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) a[u] = fabs(__ldg(x + (i + u * step) * k + c));
+      for (int u = 0; u < 4; ++u) a[u] = abs_key(__ldg(x + (i + u * step) * k + c));
 #pragma unroll
       for (int u = 0; u < 4; ++u)
         if (a[u] > best) {
@@ -96,7 +153,7 @@ __global__ void __launch_bounds__(kNaThreads) k_argmax_abs_rows(const double* __
         }
     }
     for (; i < n; i += step) {
-      const double a = fabs(__ldg(x + i * k + c));
+      const long long a = abs_key(__ldg(x + i * k + c));
       if (a > best) {
         best = a;
         bi = i;
@@ -128,17 +185,19 @@ __global__ void __launch_bounds__(kNaThreads) k_argmax_abs_rows(const double* __
   if (!last) return;
   __threadfence();
   if (t < k) {
-    double b = -1.0;
+    long long b = -1;
     long long ib = -1;
     for (int blk = 0; blk < static_cast<int>(gridDim.x); ++blk) {
-      const double a = __ldcg(&s->val[static_cast<int64_t>(blk) * kNoAllocMaxCols + t]);
+      const long long a = __ldcg(&s->val[static_cast<int64_t>(blk) * kNoAllocMaxCols + t]);
       const long long i = __ldcg(&s->idx[static_cast<int64_t>(blk) * kNoAllocMaxCols + t]);
       if (better(a, i, b, ib)) {
         b = a;
         ib = i;
       }
     }
-    s->sign[t] = (ib >= 0 && signbit(x[ib * k + t])) ? -1.0 : 1.0;
+    // Rust f64::signum: -1 for negatives and -0.0, NaN (never flipped) for NaN
+    const double v = ib >= 0 ? x[ib * k + t] : 1.0;
+    s->sign[t] = (!isnan(v) && signbit(v)) ? -1.0 : 1.0;
   }
   if (t == 0) s->ticket = 0u;
 }

@@ -1,5 +1,8 @@
 """The CPU oracle pinned against the crate's golden fixtures (the same
 tolerances as tests/integration/test_comp_*.rs of the reference)."""
+import math
+import struct
+
 import numpy as np
 import pytest
 
@@ -126,6 +129,48 @@ def test_oracle_sign_convention():
     x = np.array([[1.0, -3.0], [-2.0, 3.0], [0.5, 1.0]])
     O.normalize_signs(x)
     assert x[1, 0] == 2.0 and x[0, 1] == 3.0  # first max-|.| entry made positive
+
+
+def _rust_total_cmp_key(v: float) -> int:
+    # f64::total_cmp: bits as i64, negative values with the magnitude bits flipped
+    (b,) = struct.unpack("<q", struct.pack("<d", v))
+    return b ^ ((b >> 63) & 0x7FFFFFFFFFFFFFFF)
+
+
+def _rust_column_sign(col) -> float:
+    # src/scaling.rs:64-69: reduce(|a, b| if |b|.total_cmp(|a|).is_gt() { b } else { a }).signum()
+    best = None
+    for b in col:
+        if best is None or _rust_total_cmp_key(abs(b)) > _rust_total_cmp_key(abs(best)):
+            best = b
+    if best is None:
+        return 1.0
+    if math.isnan(best):
+        return math.nan
+    return math.copysign(1.0, best)
+
+
+def test_oracle_sign_rule_matches_total_cmp_reduce():
+    nan_a = struct.unpack("<d", struct.pack("<Q", 0x7FF8000000000001))[0]
+    nan_b = struct.unpack("<d", struct.pack("<Q", 0xFFF8000000000002))[0]  # larger payload, sign bit set
+    cols = [
+        [1.0, -3.0, 3.0, 0.5],            # tie +-3: the first (negative) wins -> flip
+        [-0.0, 0.0, -0.0],                # all zeros: first (-0.0) -> signum -1 -> flip
+        [-2.0, math.nan, -7.0],           # NaN ranks above every finite value -> never flipped
+        [-math.inf, 5.0, -1.0],           # -inf is the maximum -> flip
+        [-4.0, nan_a, nan_b, -9.0],       # NaNs rank by payload (|.| clears the sign bit)
+        [0.25, -0.5, 0.5],
+    ]
+    rng = np.random.default_rng(3)
+    cols += [list(rng.standard_normal(17)) for _ in range(5)]
+    for col in cols:
+        x = np.array(col, dtype=np.float64)[:, None].copy()
+        O.normalize_signs(x)
+        flipped = not (_rust_column_sign(col) >= 0.0 or math.isnan(_rust_column_sign(col)))
+        expect = -np.array(col) if flipped else np.array(col)
+        got = x[:, 0]
+        same = (got.view(np.uint64) == expect.view(np.uint64)) | (np.isnan(got) & np.isnan(expect))
+        assert same.all(), (col, got, expect)
 
 
 def test_oracle_errors():

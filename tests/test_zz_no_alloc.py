@@ -5,7 +5,9 @@ allocate device memory (a process whose HBM is reserved by another allocator,
 or a latency-bound loop on a shared device).  Its temporaries live in a static
 device array shared by every call, so these tests run it twice in a row on
 different shapes: what the first call leaves behind must not change the
-second call's result.  Sign flips are exact, so results must be bit-identical.
+second call's result.  Sign flips are exact, so results must be bit-identical,
+with each other and with the CPU oracle's restatement of the crate's rule
+(|x| ranked by f64::total_cmp, so a NaN maximum leaves its column unflipped).
 
 This file is collected last on purpose: it must pass alone in a fresh process
 and after every other test.
@@ -28,6 +30,19 @@ def _block(torch, n, k, seed):
     return x
 
 
+def _oracle(x_host):
+    from oracle import spectral_oracle as O
+    y = np.array(x_host, dtype=np.float64, copy=True)
+    O.normalize_signs(y)
+    return y
+
+
+def _bits_equal(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    return bool(np.all((a.view(np.uint64) == b.view(np.uint64)) | (np.isnan(a) & np.isnan(b))))
+
+
 def _run_both(ctx, torch, x):
     n, k = x.shape
     ref = x.clone()
@@ -45,6 +60,7 @@ def test_noalloc_matches_allocating_entry_twice(gpu_ctx):
         x = _block(torch, n, k, seed=11 + call)
         ref, out = _run_both(gpu_ctx, torch, x)
         assert torch.equal(ref, out), f"call {call}: n={n} k={k}"
+        assert _bits_equal(out.cpu().numpy(), _oracle(x.cpu().numpy())), f"call {call}: oracle"
         # the first entry of largest |x| in column 0 ends up positive
         col0 = x[:, 0].abs()
         first = int(torch.nonzero(col0 == col0.max())[0])
@@ -83,3 +99,37 @@ def test_noalloc_rejects_columns_beyond_scratch(gpu_ctx):
     ref, out = _run_both(gpu_ctx, torch, y)
     assert torch.equal(ref, out)
     assert np.all(np.isfinite(out.cpu().numpy()))
+
+
+def test_noalloc_nan_column_follows_total_cmp(gpu_ctx):
+    """A NaN outranks every finite |x| in the crate's reduce, and signum(NaN)
+    is not negative: the column keeps its signs although its largest finite
+    entry is negative.  Both entry points, twice in a row, against the oracle."""
+    import torch
+    x = _block(torch, 3_000, 4, seed=21)
+    x[50, 1] = -1.0e6        # largest finite entry of column 1, negative
+    x[2_000, 1] = float("nan")
+    x[10, 2] = -float("inf")  # -inf is column 2's maximum: flipped
+    host = x.cpu().numpy()
+    expect = _oracle(host)
+    assert expect[50, 1] == -1.0e6 and expect[10, 2] == float("inf")
+    for _ in range(2):
+        ref, out = _run_both(gpu_ctx, torch, x)
+        assert _bits_equal(ref.cpu().numpy(), expect)
+        assert _bits_equal(out.cpu().numpy(), expect)
+
+
+def test_noalloc_second_context_same_device(gpu_ctx):
+    """A second library context on the same device shares the device's static
+    array (same CUDA context); its calls agree with the first context's."""
+    import torch
+    from spectral_init_b200 import Context
+    other = Context(0)
+    x = _block(torch, 70_001, 5, seed=33)
+    a = x.clone()
+    b = x.clone()
+    torch.cuda.synchronize()
+    gpu_ctx.check(gpu_ctx.lib.si_normalize_signs_noalloc(gpu_ctx.ptr, a.data_ptr(), 70_001, 5))
+    other.check(other.lib.si_normalize_signs_noalloc(other.ptr, b.data_ptr(), 70_001, 5))
+    assert torch.equal(a, b)
+    assert _bits_equal(a.cpu().numpy(), _oracle(x.cpu().numpy()))
