@@ -75,7 +75,10 @@ typedef struct si_config {
   int32_t rsvd_nbiter;       /* <= 0 = 2 (src/solvers/rsvd.rs:123-126)           */
   int32_t max_iterations;    /* <= 0 = crate caps (300 first pass, 1000 restarts)  */
   int32_t learned_filter;    /* 1: also apply the Chebyshev start filter to a learned block */
-  double tol;                /* <= 0 = 1e-5 (src/metrics.rs:30,40)                 */
+  double tol;                /* LOBPCG convergence tolerance; <= 0 = 1e-5, the crate's
+                                LOBPCG_ACCEPT_TOL (src/metrics.rs:40).  Smaller values
+                                give more accurate pairs; the level-1/3 residual gate
+                                stays 1e-5 (src/metrics.rs:30)                       */
   double mixed_switch_tol;   /* mixed mode: f32 phase stops at this residual; <=0 auto */
 } si_config;
 
@@ -232,7 +235,11 @@ si_status si_normalize_signs(si_ctx* ctx, double* coords, uint64_t n, uint32_t k
  * 513 KiB that every device loading the library holds until exit, which
  * limits k to 64 columns (larger k returns SI_INVALID_ARGUMENT); n is
  * unbounded.  The first call on a device looks up that array's device
- * address, so make it before any stream capture.  All calls on a device share
+ * address, so make it before any stream capture; the address is kept per CUDA
+ * context, so after the device's context is re-created (cudaDeviceReset) the
+ * next call looks it up again.  A column whose largest |x| (ranked as the
+ * crate's f64::total_cmp ranks it, NaN highest) is a NaN keeps its signs, as
+ * in the crate and in si_normalize_signs.  All calls on a device share
  * the array: calls that overlap on the GPU race and must be serialised by the
  * caller.  Returns after the stream has finished the work. */
 si_status si_normalize_signs_noalloc(si_ctx* ctx, double* coords, uint64_t n, uint32_t k);

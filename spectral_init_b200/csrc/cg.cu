@@ -176,7 +176,7 @@ int cg_grid(const Exec& ex, int64_t items) {
 }  // namespace
 
 int cg_solve_block_dev(const Exec& ex, const OpDev& M, const double* b, double* y, int m, int ld, int64_t n,
-                       double rtol, int maxit, CgWork& w) {
+                       double rtol, int maxit, CgWork& w, bool* converged) {
   SI_REQUIRE(m >= 1 && m <= MAXM && ld >= m, SI_INVALID_ARGUMENT, "cg: block width");
   const size_t sz = static_cast<size_t>(n) * ld;
   if (w.r.size() < sz) {
@@ -217,7 +217,16 @@ int cg_solve_block_dev(const Exec& ex, const OpDev& M, const double* b, double* 
     int act = 0;
     SI_CUDA(cudaMemcpyAsync(&act, &sc->n_active, sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
     SI_CUDA(cudaStreamSynchronize(ex.stream));
-    if (act == 0) break;
+    if (act == 0) {
+      if (converged != nullptr) *converged = true;
+      return it;
+    }
+  }
+  if (converged != nullptr) {
+    int act = 1;
+    SI_CUDA(cudaMemcpyAsync(&act, &sc->n_active, sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
+    *converged = act == 0;
   }
   return it;
 }

@@ -13,6 +13,7 @@
 // their first instruction.
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstddef>
 #include <cstring>
 #include <numeric>
@@ -359,7 +360,11 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
     set_column_normalized_dev<double>(ex, s.gw, s.X.get(), ld, n, sqrt_deg);
   }
 
-  const double tol32 = static_cast<double>(static_cast<float>(LOBPCG_ACCEPT_TOL));  // linfa takes tol as f32
+  // LOBPCG convergence tolerance: the crate's LOBPCG_ACCEPT_TOL (1e-5) unless
+  // the caller asks for another (si_config.tol); linfa takes it as f32.  The
+  // level gate after the solve stays the crate's LOBPCG_QUALITY_THRESHOLD.
+  const double accept_tol = cfg.tol > 0.0 ? cfg.tol : LOBPCG_ACCEPT_TOL;
+  const double tol32 = static_cast<double>(static_cast<float>(accept_tol));
   std::vector<int> all_cols(m);
   std::iota(all_cols.begin(), all_cols.end(), 0);
 
@@ -394,6 +399,15 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
   for (int restart = 0; restart <= MAX_WARM_RESTARTS; ++restart) {
     int cap = restart == 0 ? LOBPCG_INITIAL_MAXITER_CAP : LOBPCG_RESTART_MAXITER_CAP;
     if (cfg.max_iterations > 0) cap = cfg.max_iterations;
+    if (learned && restart == 0) {
+      // test seam: SPECTRAL_INIT_LEARNED_MAXITER caps the pass that starts
+      // from the learned block, so that tests can make it stall and exercise
+      // the fallback to the random start
+      if (const char* e = std::getenv("SPECTRAL_INIT_LEARNED_MAXITER")) {
+        const int v = std::atoi(e);
+        if (v > 0) cap = v;
+      }
+    }
     const int maxiter = static_cast<int>(std::min<int64_t>(5 * n, cap));
     CoreOutcome o = lobpcg_core<double>(ex, A, s, k, tol32, maxiter, false, 1e-14, false, st.spmm_calls);
     st.iterations += o.iterations;
@@ -401,7 +415,7 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
     bool accept = o.status == ST_CONVERGED;
     if (!accept) {
       accept = true;
-      for (int c = 0; c < k; ++c) accept = accept && (o.best_rnorm[c] < LOBPCG_ACCEPT_TOL);
+      for (int c = 0; c < k; ++c) accept = accept && (o.best_rnorm[c] < accept_tol);
     }
     if (!accept && learned && restart == 0) {
       // the learned block stalled: start over from the random block
@@ -424,7 +438,7 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
     const std::vector<double> res = eigenpair_residuals_dev(ex, op, s.X.get(), ld, vals, k, DBL_EPSILON);
     ++st.spmm_calls;
     bool ok = true;
-    for (int c = 0; c < k; ++c) ok = ok && (res[c] < LOBPCG_ACCEPT_TOL);
+    for (int c = 0; c < k; ++c) ok = ok && (res[c] < accept_tol);
     if (ok) {
       out.k = k;
       out.vals.assign(vals.begin(), vals.begin() + k);
@@ -479,7 +493,9 @@ bool sinv_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64
   int inner = 0;
   const int cg_cap = static_cast<int>(std::min<int64_t>(SINV_CG_MAXIT, 10 * n + 10));
   const std::function<void(const double*, double*)> apply = [&](const double* x, double* y) {
-    inner += cg_solve_block_dev(ex, M, x, y, m, ld, n, SINV_CG_RTOL, cg_cap, cw);
+    bool conv = true;
+    inner += cg_solve_block_dev(ex, M, x, y, m, ld, n, SINV_CG_RTOL, cg_cap, cw, &conv);
+    if (!conv) ++st.sinv_cg_capped;
   };
   const double tol32 = static_cast<double>(static_cast<float>(SINV_LINFA_TOL));
   const int maxiter = static_cast<int>(std::min<int64_t>(5 * n, 300));
@@ -560,6 +576,11 @@ int rsvd_k_sub(int64_t n, int rank) {
 
 }  // namespace
 
+int rsvd_width(int64_t n, int n_components, int oversampling) {
+  const int rank = n_components + 1;
+  return oversampling < 0 ? rsvd_k_sub(n, rank) : static_cast<int>(std::min<int64_t>(rank + oversampling, n));
+}
+
 void rsvd_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64_t seed, int oversampling, int nbiter,
                     EigenResult& out, SolverStats& st) {
   // row partition for the tiled SpMM (built once per solve when absent)
@@ -573,8 +594,12 @@ void rsvd_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64
   SI_REQUIRE(n_components > 0 && n_components < n, SI_INVALID_ARGUMENT, "rsvd: need 0 < n_components < n");
   const int rank = n_components + 1;
   SI_REQUIRE(rank <= MAXM, SI_INVALID_ARGUMENT, "rsvd: n_components + 1 must be <= 16");
-  int K = oversampling < 0 ? rsvd_k_sub(n, rank) : static_cast<int>(std::min<int64_t>(rank + oversampling, n));
-  K = std::min(K, SMAX);  // device subspace cap
+  const int K = rsvd_width(n, n_components, oversampling);
+  SI_REQUIRE(K <= SMAX, SI_INVALID_ARGUMENT,
+             "rsvd: subspace width K = " + std::to_string(K) + " (n_components + 1 + oversampling" +
+                 (oversampling < 0 ? std::string(", the crate's default oversampling max(n/10, rank, 5)") : "") +
+                 ") exceeds the device limit of " + std::to_string(SMAX) + "; pass oversampling <= " +
+                 std::to_string(SMAX - rank));
   if (nbiter <= 0) nbiter = 2;
   const int ld = K <= 4 ? 4 : (K <= 8 ? 8 : (K <= 16 ? 16 : K));
   GramWork gw;
@@ -671,15 +696,25 @@ void solve_eigenproblem_dev(const Exec& ex, const OpDev& op_in, int n_components
   }
   if (want(2)) {
     EigenResult r;
+    const int capped0 = st.sinv_cg_capped;
     if (sinv_solve_dev(ex, op, n_components, seed, sqrt_deg, cfg, r, st)) {
       const double q = max_eigenpair_residual_dev(ex, op, r);
-      if (q < SINV_LOBPCG_QUALITY_THRESHOLD || fl == 2) {
+      if (q < SINV_LOBPCG_QUALITY_THRESHOLD || (fl == 2 && st.sinv_cg_capped == capped0)) {
         st.level = 2;
         st.max_residual = q;
         out = std::move(r);
         return;
       }
     }
+    // The crate applies (L + eps I)^-1 with a sparse Cholesky factor (exact to
+    // rounding); here each application is an inner CG with an iteration cap.
+    // A forced level 2 whose inner solves hit the cap and did not pass the
+    // gate reports that instead of returning an unconverged result.
+    SI_REQUIRE(!(fl == 2 && st.sinv_cg_capped > capped0), SI_ITERATION_CAP,
+               "sinv: " + std::to_string(st.sinv_cg_capped - capped0) +
+                   " inner CG solve(s) of (L + 1e-4 I) y = x stopped at the cap of " + std::to_string(SINV_CG_MAXIT) +
+                   " iterations before relative residual " + std::to_string(SINV_CG_RTOL) +
+                   " and the level-2 result failed its residual gate");
   }
   if (want(3)) {
     EigenResult r;
@@ -693,7 +728,10 @@ void solve_eigenproblem_dev(const Exec& ex, const OpDev& op_in, int n_components
       }
     }
   }
-  if (want(4)) {
+  // Level 4 needs its subspace (K = n_components + 1 + oversampling) within the
+  // device limit; inside the chain a wider default subspace skips to level 5
+  // (a forced level 4 reports the limit as an error instead).
+  if (want(4) && (fl == 4 || rsvd_width(n, n_components, cfg.rsvd_oversampling) <= SMAX)) {
     EigenResult r;
     rsvd_solve_dev(ex, op, n_components, seed, cfg.rsvd_oversampling, cfg.rsvd_nbiter, r, st);
     const double q = max_eigenpair_residual_dev(ex, op, r);

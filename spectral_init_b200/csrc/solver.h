@@ -36,6 +36,7 @@ struct SolverStats {
   int restarts = 0;
   int fp32_iterations = 0;
   int spmm_calls = 0;
+  int sinv_cg_capped = 0;  // level-2 inner solves that stopped at their iteration cap
   double max_residual = 0.0;
 };
 
@@ -51,7 +52,12 @@ struct EigenResult {
 bool lobpcg_solve_dev(const Exec& ex, const OpDev& op, int n_components, uint64_t seed, bool regularize,
                       const double* sqrt_deg, const SolverConfig& cfg, EigenResult& out, SolverStats& st);
 
-// rsvd_solve (src/solvers/rsvd.rs:135-213).
+// Subspace width K of rsvd_solve: n_components + 1 + oversampling, or the
+// crate's default oversampling (src/solvers/rsvd.rs:84-87) when it is < 0.
+int rsvd_width(int64_t n, int n_components, int oversampling);
+
+// rsvd_solve (src/solvers/rsvd.rs:135-213).  K above the device small-problem
+// limit (64) is an SI_INVALID_ARGUMENT error, not a silently narrower subspace.
 void rsvd_solve_dev(const Exec& ex, const OpDev& op, int n_components, uint64_t seed, int oversampling, int nbiter,
                     EigenResult& out, SolverStats& st);
 

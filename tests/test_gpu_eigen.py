@@ -148,10 +148,22 @@ def test_lobpcg_precondition_failures_return_none(gpu_ctx):
 @pytest.mark.parametrize("ds", ["blobs_connected_200", "blobs_connected_2000", "moons_200", "circles_300",
                                 "near_dupes_100"])
 def test_rsvd_sanity(gpu_ctx, ds):
+    """test_comp_d_rsvd.rs sanity tolerances (5e-1).  The crate's default width
+    K = rank + max(n/10, rank, 5) (src/solvers/rsvd.rs:84-87) is honoured where
+    it fits the device limit of 64 columns; above it the call is an explicit
+    SI_INVALID_ARGUMENT naming the limit, and the widest allowed subspace runs."""
     import spectral_init_b200 as si
+    from spectral_init_b200.api import InvalidArgument
     lap = load_csr(ds, "comp_b_laplacian.npz")
     ref = load_npz(ds, "comp_d_eigensolver.npz")["eigenvalues"]
-    vals, vecs = si.rsvd_solve(lap, 2, 42, ctx=gpu_ctx)
+    n = lap.shape[0]
+    default_k = 3 + min(max(n // 10, 5), n - 3)
+    over = None
+    if default_k > 64:
+        with pytest.raises(InvalidArgument, match="64"):
+            si.rsvd_solve(lap, 2, 42, ctx=gpu_ctx)
+        over = 64 - 3
+    vals, vecs = si.rsvd_solve(lap, 2, 42, oversampling=over, ctx=gpu_ctx)
     for i in range(2):
         assert abs(vals[i + 1] - ref[i + 1]) < 5e-1
         assert resid(lap, vecs[:, i + 1], vals[i + 1]) < 5e-1
