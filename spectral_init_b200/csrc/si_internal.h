@@ -27,6 +27,8 @@ struct GraphDev {
   const float* data = nullptr;
 };
 
+struct RowBlocks;
+
 // Sparse operator y = diag * x + sum_j v_ij x_j on the device.
 struct OpDev {
   int64_t n = 0, nnz = 0;
@@ -44,6 +46,9 @@ struct OpDev {
   const int64_t* gather_blocks = nullptr;
   const uint64_t* gather_ptr = nullptr;
   int64_t n_gather_blocks = 0;
+  // panel partition (about kPanelBlockNnz entries a block) and its per-block
+  // x windows, built on demand for each window size (null: not available)
+  const RowBlocks* panels = nullptr;
 };
 
 constexpr int kSpmmBlockNnz = 1024;   // target entries per row block
@@ -51,13 +56,25 @@ constexpr int kSpmmBlockCap = 2048;   // entries a block may hold in shared memo
 constexpr int kSpmmBlockRows = 1024;  // rows a block may hold in shared memory
 constexpr int kGatherBlockNnz = 384;  // target entries per TMA-gather block
 constexpr int kGatherCap = 512;       // entries a TMA-gather block may stage
+constexpr int kPanelBlockNnz = 4096;  // target entries per panel block
+constexpr int kPanelBytes = 200 * 1024;  // shared memory of the staged x window
+
+// x window of the panel SpMM for one window size: block b gathers x rows
+// [w0[b], w0[b] + W) from shared memory.
+struct PanelWindows {
+  int W = 0;
+  DevBuf<int64_t> w0;
+};
 
 // Row partition of an operator for the tiled SpMM (device array of
 // n_blocks + 1 row starts, owned by the caller).
 struct RowBlocks {
-  DevBuf<int64_t> starts, gstarts;
-  DevBuf<uint64_t> ptrs, gptrs;
-  int64_t n_blocks = 0, n_gblocks = 0;
+  DevBuf<int64_t> starts, gstarts, pstarts;
+  DevBuf<uint64_t> ptrs, gptrs, pptrs;
+  int64_t n_blocks = 0, n_gblocks = 0, n_pblocks = 0;
+  // windows of the panel SpMM, one entry per window size used (built lazily
+  // by the first SpMM that needs them outside stream capture)
+  mutable std::vector<PanelWindows> windows;
   void attach(OpDev& op) const {
     op.row_blocks = starts.get();
     op.block_ptr = ptrs.get();
@@ -65,6 +82,7 @@ struct RowBlocks {
     op.gather_blocks = gstarts.get();
     op.gather_ptr = gptrs.get();
     op.n_gather_blocks = n_gblocks;
+    op.panels = this;
   }
 };
 void make_row_blocks(const Exec& ex, const OpDev& op, RowBlocks& rb);
@@ -212,8 +230,9 @@ struct CgWork {
   DevBuf<unsigned> counter;
   DevBuf<unsigned char> scal;
 };
+// *converged (optional) tells whether every column reached rtol within maxit.
 int cg_solve_block_dev(const Exec& ex, const OpDev& M, const double* b, double* y, int m, int ld, int64_t n,
-                       double rtol, int maxit, CgWork& w);
+                       double rtol, int maxit, CgWork& w, bool* converged = nullptr);
 
 // ---- noalloc.cu -----------------------------------------------------------------
 // Sign normalisation of a contiguous f64 block [n x k] with all temporaries in

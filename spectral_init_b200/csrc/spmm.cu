@@ -391,6 +391,208 @@ __global__ void k_row_blocks(int64_t n, const uint64_t* __restrict__ indptr, int
   }
 }
 
+// ---------------------------------------------------------------------------
+// Panel SpMM: the x rows a run of rows gathers from are staged once in shared
+// memory.  Graph orders in which each node's neighbours sit near it (kNN
+// graphs of clustered data in cluster order, locality orders) give each block
+// of ~kPanelBlockNnz entries a contiguous window of W x rows that holds most
+// of its column indices; the block's gathers then hit shared memory (several
+// entries per clock per SM) instead of issuing one scattered L2 request each,
+// which is what bounds the direct kernels.  Entries outside the window fall
+// back to a global gather.
+
+// Window plan: for each panel block, the start w0 of the W-row window that
+// holds the most of its column indices (histogram over bins of `bin` rows,
+// best run of W / bin bins, ties to the lowest start), clamped to [0, n - W].
+constexpr int kPanelBins = 4096;
+constexpr int kPlanThreads = 256;
+
+__global__ void __launch_bounds__(kPlanThreads) k_panel_windows(int64_t n, const uint64_t* __restrict__ indptr,
+                                                                const uint32_t* __restrict__ indices,
+                                                                const int64_t* __restrict__ prow, int64_t nblk, int W,
+                                                                int bin, int nbins, int64_t* __restrict__ w0) {
+  __shared__ int hist[kPanelBins];
+  __shared__ long long best_key[kPlanThreads / 32];
+  const int tid = threadIdx.x;
+  const int wb = max(W / bin, 1);  // window length in bins
+  const int nstart = max(nbins - wb + 1, 1);
+  for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
+    for (int i = tid; i < nbins; i += kPlanThreads) hist[i] = 0;
+    __syncthreads();
+    const uint64_t p0 = indptr[prow[b]], p1 = indptr[prow[b + 1]];
+    for (uint64_t q = p0 + tid; q < p1; q += kPlanThreads) {
+      const int bi = static_cast<int>(__ldg(indices + q) / static_cast<uint32_t>(bin));
+      atomicAdd(&hist[min(bi, nbins - 1)], 1);
+    }
+    __syncthreads();
+    // each thread scans a contiguous range of starts with a sliding sum;
+    // key = count * 2^32 + (2^32 - 1 - start): max picks the most entries, then the lowest start
+    const int per = (nstart + kPlanThreads - 1) / kPlanThreads;
+    const int s0 = tid * per, s1 = min(s0 + per, nstart);
+    long long key = -1;
+    if (s0 < s1) {
+      int sum = 0;
+      for (int i = s0; i < min(s0 + wb, nbins); ++i) sum += hist[i];
+      for (int st = s0; st < s1; ++st) {
+        if (st > s0) sum += (st + wb - 1 < nbins ? hist[st + wb - 1] : 0) - hist[st - 1];
+        const long long k = (static_cast<long long>(sum) << 32) | static_cast<long long>(0xffffffffu - st);
+        key = max(key, k);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) key = max(key, __shfl_xor_sync(0xffffffffu, key, o));
+    if ((tid & 31) == 0) best_key[tid >> 5] = key;
+    __syncthreads();
+    if (tid == 0) {
+      long long k = best_key[0];
+      for (int w = 1; w < kPlanThreads / 32; ++w) k = max(k, best_key[w]);
+      const int64_t st = static_cast<int64_t>(0xffffffffu - static_cast<unsigned>(k & 0xffffffffLL));
+      int64_t start = st * bin;
+      start = min(start, max(n - static_cast<int64_t>(W), int64_t(0)));
+      w0[b] = max(start, int64_t(0));
+    }
+    __syncthreads();
+  }
+}
+
+// x row of LD elements from the shared-memory window (16-byte vector loads).
+template <class XT, int LD>
+__device__ __forceinline__ void smem_row(const XT* p, double (&v)[LD]) {
+  if constexpr (std::is_same<XT, float>::value) {
+#pragma unroll
+    for (int q = 0; q < LD / 4; ++q) {
+      const float4 t = reinterpret_cast<const float4*>(p)[q];
+      v[4 * q + 0] = t.x;
+      v[4 * q + 1] = t.y;
+      v[4 * q + 2] = t.z;
+      v[4 * q + 3] = t.w;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < LD / 2; ++q) {
+      const double2 t = reinterpret_cast<const double2*>(p)[q];
+      v[2 * q + 0] = t.x;
+      v[2 * q + 1] = t.y;
+    }
+  }
+}
+
+// One row by a group of G lanes, gathers from the window [w, w + wn) when the
+// column falls inside it (spmm_row otherwise).
+template <class VT, class XT, int LD, int G>
+__device__ __forceinline__ void spmm_row_panel(int64_t row, uint64_t s, uint64_t e, const uint32_t* __restrict__ idx,
+                                               const VT* __restrict__ val, double diag, const XT* __restrict__ x,
+                                               const XT* panel, uint32_t w, uint32_t wn, XT* __restrict__ y,
+                                               const Epilogue<XT>& ep, int sub, unsigned mask, bool writer) {
+  constexpr int W = GroupReduce<LD, G>::W;
+  constexpr int U = (LD >= 16) ? 4 : 8;
+  const int obase = GroupReduce<LD, G>::base_of(sub);
+  double own[W], addz[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) {
+    own[c] = 0.0;
+    addz[c] = 0.0;
+    if (writer) {
+      const int64_t off = row * LD + obase + c;
+      own[c] = diag * static_cast<double>(x[off]);
+      if (ep.z1) addz[c] = ep.beta * static_cast<double>(ep.z1[off]);
+      if (ep.z2) addz[c] = fma(ep.gamma, static_cast<double>(ep.z2[off]), addz[c]);
+      if (ep.z3) addz[c] = fma(ep.delta, static_cast<double>(ep.z3[off]), addz[c]);
+    }
+  }
+  double acc[LD];
+#pragma unroll
+  for (int c = 0; c < LD; ++c) acc[c] = 0.0;
+  for (uint64_t b0 = s + sub; b0 < e; b0 += static_cast<uint64_t>(G) * U) {
+    uint32_t jj[U];
+    double vv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t k = b0 + static_cast<uint64_t>(u) * G;
+      const bool ok = k < e;
+      jj[u] = ok ? ld_stream(idx + k) : 0u;
+      vv[u] = ok ? static_cast<double>(ld_stream(val + k)) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (b0 + static_cast<uint64_t>(u) * G < e) {
+        double xr[LD];
+        const uint32_t d = jj[u] - w;
+        if (d < wn) smem_row<XT, LD>(panel + static_cast<size_t>(d) * LD, xr);
+        else RowLoad<XT, LD>::run(x + static_cast<int64_t>(jj[u]) * LD, xr);
+#pragma unroll
+        for (int c = 0; c < LD; ++c) acc[c] = fma(vv[u], xr[c], acc[c]);
+      }
+    }
+  }
+  const int base = GroupReduce<LD, G>::run(acc, sub, mask);
+  if (writer) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      const int64_t off = row * LD + base + c;
+      y[off] = static_cast<XT>(fma(ep.alpha, own[c] + acc[c], addz[c]));
+    }
+  }
+}
+
+template <class XT, int LD>
+constexpr int panel_threads() {
+  return LD * sizeof(XT) <= 16 ? 1024 : 512;
+}
+
+template <class XT, int LD>
+constexpr int panel_rows() {
+  return (kPanelBytes / (LD * static_cast<int>(sizeof(XT)))) / 64 * 64;
+}
+
+// Persistent CTAs (one per SM): CTA c walks panel blocks [c*nblk/grid,
+// (c+1)*nblk/grid); consecutive blocks with the same window form one run whose
+// rows are spread over the CTA's row groups; the window is reloaded (between
+// two CTA barriers) only when a run's window differs from the one held.
+template <class VT, class XT, int LD, int G, int NT>
+__global__ void __launch_bounds__(NT, 1) k_spmm_panel(int64_t n, const uint64_t* __restrict__ indptr,
+                                                      const uint32_t* __restrict__ indices,
+                                                      const VT* __restrict__ vals, const int64_t* __restrict__ prow,
+                                                      const int64_t* __restrict__ pw0, int64_t nblk, double diag,
+                                                      const XT* __restrict__ x, XT* __restrict__ y, Epilogue<XT> ep,
+                                                      const int* __restrict__ stop) {
+  if (stop != nullptr && *stop != 0) return;
+  constexpr int WR = panel_rows<XT, LD>();
+  extern __shared__ __align__(16) unsigned char panel_raw[];
+  XT* panel = reinterpret_cast<XT*>(panel_raw);
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int sub = lane & (G - 1);
+  const unsigned mask = group_mask<G>(lane);
+  const bool writer = group_writer<LD, G>(sub);
+  const int group = tid / G;
+  constexpr int NG = NT / G;
+  const int64_t b_lo = nblk * blockIdx.x / gridDim.x;
+  const int64_t b_hi = nblk * (blockIdx.x + 1) / gridDim.x;
+  int64_t held = -1;
+  for (int64_t b = b_lo; b < b_hi;) {
+    const int64_t w = pw0[b];
+    int64_t be = b + 1;
+    while (be < b_hi && pw0[be] == w) ++be;
+    const int64_t r0 = prow[b], r1 = prow[be];
+    const uint32_t wn = static_cast<uint32_t>(min(static_cast<int64_t>(WR), n - w));
+    if (w != held) {
+      __syncthreads();  // every row of the previous run is done with the old window
+      constexpr int VEC = 16 / sizeof(XT);
+      const int64_t nvec = static_cast<int64_t>(wn) * LD / VEC;
+      const uint4* src = reinterpret_cast<const uint4*>(x + w * LD);
+      uint4* dst = reinterpret_cast<uint4*>(panel);
+      for (int64_t i = tid; i < nvec; i += NT) dst[i] = __ldcg(src + i);
+      __syncthreads();
+      held = w;
+    }
+    for (int64_t row = r0 + group; row < r1; row += NG)
+      spmm_row_panel<VT, XT, LD, G>(row, indptr[row], indptr[row + 1], indices, vals, diag, x, panel,
+                                    static_cast<uint32_t>(w), wn, y, ep, sub, mask, writer);
+    b = be;
+  }
+}
+
 // Generic kernel: any row stride ld, first k columns, four columns per pass.
 template <class VT, class XT, int G>
 __global__ void __launch_bounds__(256) k_spmm_generic(int64_t n, const uint64_t* __restrict__ indptr,
@@ -685,10 +887,66 @@ void launch_tiled(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, 
   SI_LAUNCH_CHECK();
 }
 
+// Windows of the panel SpMM for window size W (built on first use, outside
+// stream capture; null when the operator has no panel partition or when the
+// windows would have to be built inside a capture).
+const int64_t* panel_windows(const Exec& ex, const OpDev& op, int W) {
+  if (op.panels == nullptr || op.panels->n_pblocks <= 0 || W <= 0) return nullptr;
+  for (const PanelWindows& pw : op.panels->windows)
+    if (pw.W == W) return pw.w0.get();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  SI_CUDA(cudaStreamIsCapturing(ex.stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return nullptr;
+  int64_t bin = std::max<int64_t>(1, (W + 7) / 8);
+  int64_t nbins = (op.n + bin - 1) / bin;
+  if (nbins > kPanelBins) {
+    bin = (op.n + kPanelBins - 1) / kPanelBins;
+    nbins = (op.n + bin - 1) / bin;
+  }
+  PanelWindows pw;
+  pw.W = W;
+  const int64_t nb = op.panels->n_pblocks;
+  pw.w0.alloc(static_cast<size_t>(nb), ex.stream);
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(nb, int64_t(ex.sms) * 8)));
+  k_panel_windows<<<grid, kPlanThreads, 0, ex.stream>>>(op.n, op.indptr, op.indices, op.panels->pstarts.get(), nb, W,
+                                                        static_cast<int>(bin), static_cast<int>(std::max<int64_t>(nbins, 1)),
+                                                        pw.w0.get());
+  SI_LAUNCH_CHECK();
+  op.panels->windows.push_back(std::move(pw));
+  return op.panels->windows.back().w0.get();
+}
+
+template <class VT, class XT, int LD>
+bool launch_panel(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
+                  const int* stop) {
+  constexpr int WR = panel_rows<XT, LD>();
+  constexpr int NT = panel_threads<XT, LD>();
+  constexpr int G = 4;
+  const int64_t* w0 = panel_windows(ex, op, WR);
+  if (w0 == nullptr) return false;
+  const int smem = WR * LD * static_cast<int>(sizeof(XT));
+  static std::atomic<int> ready[128];
+  const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
+  if (ready[dev] == 0) {
+    SI_CUDA(cudaFuncSetAttribute(k_spmm_panel<VT, XT, LD, G, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ready[dev] = 1;
+  }
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(op.panels->n_pblocks, int64_t(ex.sms))));
+  k_spmm_panel<VT, XT, LD, G, NT><<<grid, NT, smem, ex.stream>>>(op.n, op.indptr, op.indices, vals,
+                                                                  op.panels->pstarts.get(), w0, op.panels->n_pblocks,
+                                                                  op.diag, x, y, ep, stop);
+  SI_LAUNCH_CHECK();
+  return true;
+}
+
 // choice < 100: direct kernel with `choice` lanes per row; 100 + g: tiled kernel
 template <class VT, class XT, int LD>
 void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                   const int* stop) {
+  if (g == 300) {
+    if (launch_panel<VT, XT, LD>(ex, op, vals, x, y, ep, stop)) return;
+    g = spmm_group_lanes(op);  // no windows (inside a capture before first use): direct kernel
+  }
   switch (g) {
     case 4: launch_vec<VT, XT, LD, 4>(ex, op, vals, x, y, ep, stop); break;
     case 8: launch_vec<VT, XT, LD, 8>(ex, op, vals, x, y, ep, stop); break;
@@ -716,11 +974,12 @@ void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const 
 struct TuneKey {
   int device;
   const void* indptr;
+  const void* indices;
   int64_t n, nnz;
-  int ld, vbytes, xbytes, tiled;
+  int ld, vbytes, xbytes, tiled, panel;
   bool operator<(const TuneKey& o) const {
-    return std::tie(device, indptr, n, nnz, ld, vbytes, xbytes, tiled) <
-           std::tie(o.device, o.indptr, o.n, o.nnz, o.ld, o.vbytes, o.xbytes, o.tiled);
+    return std::tie(device, indptr, indices, n, nnz, ld, vbytes, xbytes, tiled, panel) <
+           std::tie(o.device, o.indptr, o.indices, o.n, o.nnz, o.ld, o.vbytes, o.xbytes, o.tiled, o.panel);
   }
 };
 std::mutex g_tune_mu;
@@ -736,11 +995,13 @@ int forced_choice(const OpDev& op, bool tiled) {
   const std::string v(env);
   static const std::pair<const char*, int> names[] = {{"vec4", 4},     {"vec8", 8},       {"vec16", 16},
                                                       {"vec32", 32},   {"tiled4", 104},   {"tiled8", 108},
-                                                      {"gather4", 204}, {"gather8", 208}};
+                                                      {"gather4", 204}, {"gather8", 208},
+                                                      {"panel", 300}};
   for (const auto& nm : names) {
     if (v != nm.first) continue;
     const int c = nm.second;
     if (c > 100 && c < 200 && !tiled) return 0;
+    if (c == 300 && (op.panels == nullptr || op.panels->n_pblocks <= 0)) return 0;
     if (c > 200 && !(std::is_same<VT, float>::value && std::is_same<XT, float>::value && LD == 4 &&
                      op.gather_blocks != nullptr && op.n_gather_blocks > 0))
       return 0;
@@ -753,8 +1014,9 @@ template <class VT, class XT, int LD>
 void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                 const int* stop) {
   const bool tiled = op.row_blocks != nullptr && op.n_blocks > 0;
-  const TuneKey key{ex.device, op.indptr, op.n, op.nnz, LD, static_cast<int>(sizeof(VT)),
-                    static_cast<int>(sizeof(XT)), tiled ? 1 : 0};
+  const bool panel = op.panels != nullptr && op.panels->n_pblocks > 0;
+  const TuneKey key{ex.device, op.indptr, op.indices, op.n, op.nnz, LD, static_cast<int>(sizeof(VT)),
+                    static_cast<int>(sizeof(XT)), tiled ? 1 : 0, panel ? 1 : 0};
   int g = forced_choice<VT, XT, LD>(op, tiled);
   if (g != 0) {
     launch_lanes<VT, XT, LD>(g, ex, op, vals, x, y, ep, stop);
@@ -786,6 +1048,7 @@ void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT
         cands.push_back(204);
         cands.push_back(208);
       }
+      if (op.panels != nullptr && op.panels->n_pblocks > 0) cands.push_back(300);
       for (int cand : cands) {
         launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
         SI_CUDA(cudaEventRecord(e0, ex.stream));
@@ -841,6 +1104,8 @@ void make_row_blocks(const Exec& ex, const OpDev& op, RowBlocks& rb) {
   };
   build(kSpmmBlockNnz, rb.n_blocks, rb.starts, rb.ptrs);
   build(kGatherBlockNnz, rb.n_gblocks, rb.gstarts, rb.gptrs);
+  build(kPanelBlockNnz, rb.n_pblocks, rb.pstarts, rb.pptrs);
+  rb.windows.clear();
 }
 
 int spmm_group_lanes(const OpDev& op) {

@@ -94,7 +94,8 @@ def _variant_matrix():
     return _VARIANT_CACHE["a"]
 
 
-@pytest.mark.parametrize("kernel", ["vec4", "vec8", "vec16", "vec32", "tiled4", "tiled8", "gather4", "gather8"])
+@pytest.mark.parametrize("kernel", ["vec4", "vec8", "vec16", "vec32", "tiled4", "tiled8", "gather4", "gather8",
+                                    "panel"])
 @pytest.mark.parametrize("prec", ["f32", "f64"])
 def test_spmm_every_kernel_variant(gpu_ctx, kernel, prec):
     """Each SpMM variant the autotuner can pick (SPECTRAL_INIT_SPMM_KERNEL forces
@@ -111,6 +112,55 @@ def test_spmm_every_kernel_variant(gpu_ctx, kernel, prec):
     x = np.random.default_rng(8).standard_normal((n, 4)).astype(dt)
     old = os.environ.get("SPECTRAL_INIT_SPMM_KERNEL")
     os.environ["SPECTRAL_INIT_SPMM_KERNEL"] = kernel
+    try:
+        y = op.apply(torch.from_numpy(x).cuda()).cpu().numpy()
+    finally:
+        if old is None:
+            del os.environ["SPECTRAL_INIT_SPMM_KERNEL"]
+        else:
+            os.environ["SPECTRAL_INIT_SPMM_KERNEL"] = old
+    vals = a.data.astype(np.float32).astype(np.float64) if prec == "f32" else a.data
+    av = sp.csr_matrix((vals, a.indices, a.indptr), shape=a.shape)
+    ref = x.astype(np.float64) + av @ x.astype(np.float64)
+    assert _rel(y, ref) < (2e-6 if prec == "f32" else 1e-14)
+
+
+def _clustered_matrix():
+    """120 000 rows in 10 contiguous clusters of 12 000 (about 20 entries per
+    row inside the cluster, 1 % of entries anywhere), symmetrised: the shape
+    of a kNN graph of clustered points in cluster order."""
+    if "c" not in _VARIANT_CACHE:
+        rng = np.random.default_rng(11)
+        n, size = 120_000, 12_000
+        r = np.repeat(np.arange(n), 10)
+        base = (r // size) * size
+        c = base + rng.integers(0, size, r.size)
+        far = rng.random(r.size) < 0.01
+        c[far] = rng.integers(0, n, int(far.sum()))
+        a = sp.csr_matrix((rng.uniform(0.1, 1.0, r.size), (r, c)), shape=(n, n))
+        a = (a + a.T).tocsr()
+        a.sum_duplicates()
+        a.sort_indices()
+        _VARIANT_CACHE["c"] = a
+    return _VARIANT_CACHE["c"]
+
+
+@pytest.mark.parametrize("width", [4, 8, 16])
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_spmm_panel_windows_clustered(gpu_ctx, width, prec):
+    """The panel kernel (x windows staged in shared memory, out-of-window
+    entries gathered from global memory) on a cluster-ordered matrix larger
+    than every window, for 4-, 8- and 16-wide blocks, against scipy in f64."""
+    import os
+    import torch
+    import spectral_init_b200 as si
+    a = _clustered_matrix()
+    n = a.shape[0]
+    op = si.CsrOperator(a, diag=1.0, ctx=gpu_ctx, with_f32=(prec == "f32"))
+    dt = np.float32 if prec == "f32" else np.float64
+    x = np.random.default_rng(9).standard_normal((n, width)).astype(dt)
+    old = os.environ.get("SPECTRAL_INIT_SPMM_KERNEL")
+    os.environ["SPECTRAL_INIT_SPMM_KERNEL"] = "panel"
     try:
         y = op.apply(torch.from_numpy(x).cuda()).cpu().numpy()
     finally:
