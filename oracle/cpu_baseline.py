@@ -147,3 +147,53 @@ def solve_timed(op: CpuOperator, n_components: int, seed: int, sqrt_deg, budget_
         out["seconds"] = t_filter + t_iter_total
         out["projected"] = "lower-bound"
     return out
+
+
+def laplacian_operator(indptr, indices, weights, n: int):
+    """The crate's Laplacian on the CPU (src/laplacian.rs:8-88): PythonCompat
+    degrees by the f32 column scatter in CSR order, ``inv = 1/sqrt(d)`` (0 for
+    isolated nodes), off-diagonal values ``-inv_i * w_ij * inv_j`` evaluated
+    left to right in f64 on the graph's own pattern (self loops 0), unit
+    diagonal applied implicitly.  Returns ``(CpuOperator, sqrt_deg)``."""
+    ip = np.ascontiguousarray(indptr, dtype=np.uint64)
+    ix = np.ascontiguousarray(indices, dtype=np.uint32)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    deg = np.zeros(n, dtype=np.float32)
+    load().column_sum_f32(len(ix), ix.ctypes.data, w.ctypes.data, deg.ctypes.data)
+    sq = np.sqrt(deg.astype(np.float64))
+    inv = O.inv_sqrt(sq)
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(ip.astype(np.int64)))
+    cols = ix.astype(np.int64)
+    vals = np.where(rows == cols, 0.0, (-inv[rows]) * w.astype(np.float64) * inv[cols])
+    return CpuOperator(ip, ix, vals, n, diag=1.0), sq
+
+
+def solve_measured(op: CpuOperator, n_components: int, seed: int, sqrt_deg):
+    """The crate's Level-1 solve run to completion on the CPU and timed:
+    seeded random start with the trivial-vector hint, Chebyshev filter,
+    LOBPCG with warm restarts, Rayleigh-Ritz refinement and the per-vector
+    residual check (src/solvers/lobpcg.rs:227-465), then the level gate
+    (src/metrics.rs:73-92).  Nothing is projected."""
+    stats = {}
+    t0 = time.perf_counter()
+    r = O.lobpcg_solve(op, n_components, seed, False, np.asarray(sqrt_deg, dtype=np.float64), stats=stats)
+    gate = float("nan")
+    if r is not None:
+        (vals, vecs), _ = r
+        lv = op.apply(vecs)
+        d = lv - vecs * np.asarray(vals)[None, :]
+        gate = float(np.max(np.linalg.norm(d, axis=0) / np.maximum(np.linalg.norm(vecs, axis=0), 1e-300)))
+    secs = time.perf_counter() - t0
+    return {"seconds": secs, "converged": r is not None and gate < O.LOBPCG_QUALITY_THRESHOLD,
+            "iterations": stats.get("iterations"), "restarts": stats.get("restarts"), "max_residual": gate,
+            "eigenvalues": None if r is None else [float(v) for v in r[0][0]]}
+
+
+def set_threads(t: int) -> None:
+    """Threads of the C kernels (OpenMP) and of numpy's BLAS."""
+    load().csr_set_threads(int(t))
+    try:
+        from threadpoolctl import threadpool_limits
+        threadpool_limits(int(t))
+    except Exception:
+        pass
