@@ -282,6 +282,7 @@ struct CoopTri {
   unsigned* vready;  // last step whose reflector is published
   unsigned* arrive;  // grid barrier arrivals (G per step)
   int* err;
+  uint64_t wait_ns;  // limit of every wait
 };
 
 __device__ __forceinline__ uint64_t coop_ns() {
@@ -303,13 +304,13 @@ __device__ __forceinline__ void red_release_add_u32(unsigned* p, unsigned v) {
 // One thread: wait until *p >= target, polling with a short back-off.  False
 // when the wait ran past the limit (the error word is set) or another CTA gave
 // up first.
-__device__ bool coop_wait(const unsigned* p, unsigned target, int* err) {
+__device__ bool coop_wait(const unsigned* p, unsigned target, int* err, uint64_t limit_ns) {
   if (ld_acquire_u32(p) >= target) return true;
   const uint64_t t0 = coop_ns();
   while (ld_acquire_u32(p) < target) {
     __nanosleep(32);
     if (*reinterpret_cast<volatile int*>(err) != 0) return false;
-    if (coop_ns() - t0 > kCoopWaitNs) {
+    if (coop_ns() - t0 > limit_ns) {
       atomicExch(err, 1);
       return false;
     }
@@ -365,7 +366,7 @@ __global__ void __launch_bounds__(CT_THREADS, 1) k_tridiag_coop(CoopTri p) {
         st_release_u32(p.vready, static_cast<unsigned>(j + 1));
       }
     }
-    if (tid == 0) s_ok = coop_wait(p.vready, static_cast<unsigned>(j + 1), p.err) ? 1 : 0;
+    if (tid == 0) s_ok = coop_wait(p.vready, static_cast<unsigned>(j + 1), p.err, p.wait_ns) ? 1 : 0;
     __syncthreads();
     if (!s_ok) return;
     const double tau = __ldcg(p.tau + j);
@@ -415,7 +416,7 @@ __global__ void __launch_bounds__(CT_THREADS, 1) k_tridiag_coop(CoopTri p) {
         sh[b] = share;
         __threadfence();
         red_release_add_u32(p.arrive, 1u);
-        s_ok = coop_wait(p.arrive, static_cast<unsigned>(j + 1) * static_cast<unsigned>(G), p.err) ? 1 : 0;
+        s_ok = coop_wait(p.arrive, static_cast<unsigned>(j + 1) * static_cast<unsigned>(G), p.err, p.wait_ns) ? 1 : 0;
       }
     }
     __syncthreads();
@@ -1042,6 +1043,19 @@ int smem_limit(int device, F* kernel) {
   return dyn;
 }
 
+// Limit of every wait of the single-launch tridiagonalisation: 2 s, or less
+// through SPECTRAL_INIT_COOP_WAIT_NS (a test seam: a limit of 0 makes the
+// first wait that is not already satisfied give up, which exercises the
+// recovery path -- every CTA leaves at its next wait and the multi-launch
+// steps redo the matrix).
+uint64_t coop_wait_limit_ns() {
+  const char* v = std::getenv("SPECTRAL_INIT_COOP_WAIT_NS");
+  if (v == nullptr) return kCoopWaitNs;
+  char* end = nullptr;
+  const unsigned long long x = std::strtoull(v, &end, 10);
+  return (end != v) ? static_cast<uint64_t>(std::min<unsigned long long>(x, kCoopWaitNs)) : kCoopWaitNs;
+}
+
 // SPECTRAL_INIT_TRIDIAG=steps selects the multi-launch steps for every n
 // (read on every call, so one process can exercise both paths).
 bool coop_disabled() {
@@ -1087,6 +1101,7 @@ bool tridiag_coop(const Exec& ex, double* A, int n, double* d, double* e, double
   p.vready = flags.get();
   p.arrive = flags.get() + kFlagStride;
   p.err = reinterpret_cast<int*>(flags.get() + 2 * kFlagStride);
+  p.wait_ns = coop_wait_limit_ns();
   void* args[] = {&p};
   SI_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_tridiag_coop), dim3(G), dim3(CT_THREADS), args,
                                       smem, ex.stream));

@@ -18,6 +18,8 @@
 // The Gram matrices come from the fused device pass over the blocks, so the
 // residuals never need an explicit orthogonalisation pass.
 #include <cfloat>
+#include <cstdlib>
+#include <string>
 
 #include "si_internal.h"
 
@@ -35,6 +37,17 @@ struct SmallSmem {
   double* T;  // second buffer of A for the double-buffered Jacobi
   int ld;
 };
+
+// Sweep stopping test of the Jacobi eigensolvers: the off-diagonal Frobenius
+// mass against (4 s eps)^2 times the diagonal mass.  Rounding keeps a
+// rotated s x s matrix's off-diagonal part at about eps * ||A|| per entry, so
+// a test at eps^2 alone is rarely met and runs sweeps to the cap; at this
+// level the eigenvalues are exact to rounding and the eigenvectors to
+// s eps ||A|| / gap.
+__device__ __forceinline__ double jacobi_stop2(int s) {
+  const double t = 4.0 * static_cast<double>(s) * DBL_EPSILON;
+  return t * t;
+}
 
 __device__ void cta_identity(double* V, int s, int ld) {
   for (int i = threadIdx.x; i < s * s; i += blockDim.x) V[(i / s) * ld + i % s] = (i / s == i % s) ? 1.0 : 0.0;
@@ -165,7 +178,7 @@ __device__ void cta_jacobi_db(double* A, double* V, double* A2, double* V2, int 
     }
     off = cta_sum(off, red);
     dia = cta_sum(dia, red);
-    if (!(off > DBL_EPSILON * DBL_EPSILON * dia)) break;
+    if (!(off > jacobi_stop2(s) * dia)) break;
     for (int r = 0; r < s2 - 1; ++r) {
       for (int p = threadIdx.x; p < np; p += blockDim.x) {
         int a, b;
@@ -267,7 +280,7 @@ __device__ void cta_jacobi(double* A, double* V, int s, int ld, double* red, dou
     }
     off = cta_sum(off, red);
     dia = cta_sum(dia, red);
-    if (!(off > DBL_EPSILON * DBL_EPSILON * dia)) return;
+    if (!(off > jacobi_stop2(s) * dia)) return;
     for (int r = 0; r < s2 - 1; ++r) {
       for (int p = threadIdx.x; p < np; p += blockDim.x) {
         int a, b;
@@ -334,7 +347,7 @@ __device__ void cta_jacobi(double* A, double* V, int s, int ld, double* red, dou
     }
     off = cta_sum(off, red);
     dia = cta_sum(dia, red);
-    if (!(off > DBL_EPSILON * DBL_EPSILON * dia)) break;
+    if (!(off > jacobi_stop2(s) * dia)) break;
     for (int r = 0; r < s2 - 1; ++r) {
       for (int p = threadIdx.x; p < np; p += blockDim.x) {
         int a, b;
@@ -493,7 +506,272 @@ __device__ bool cta_rr_general(const double* gb, const double* ga, int P, const 
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// The same generalised Rayleigh-Ritz for s <= 16 in one warp, in registers:
+// lane j < 16 holds column j of B (then L) and of A (then C = L^-1 A L^-T),
+// lane 16 + j holds column j of the eigenvector matrix V.  Every step is
+// lane-local arithmetic and warp shuffles; no CTA barrier is involved.
+//   * Cholesky, right-looking: at step k lane k forms column k of L, which is
+//     broadcast by shuffles, and every lane j > k updates its own column;
+//   * C = L^-1 (L^-1 A)^T (A symmetric), each lane solving for its column
+//     with L read from shared memory, the transpose through shared memory,
+//     then symmetrised;
+//   * cyclic Jacobi with the round-robin pairing of 16 columns (15 rounds of
+//     8 disjoint rotations per sweep; the round and pair indices are
+//     compile-time constants, so every register index is static): a lane
+//     exchanges its column with its partner lane for the column rotation and
+//     applies the row rotations of all 8 pairs locally.  Rotation angles as in
+//     cta_jacobi_db (f32 angle, two f64 Newton normalisation steps: every
+//     rotation exactly orthogonal, a_pq left at ~1e-7 of itself for the next
+//     sweep, never forced to zero), the same sweep stopping test;
+//   * Z = D L^-T V_sel by back substitution, one lane per selected column.
+// Padded columns (j >= s) carry B = I, A = 0 and are never selected.
+constexpr int WRR = 16;
+
+__device__ __forceinline__ double sel16(const double (&a)[WRR], int i) {
+  double v = a[0];
+#pragma unroll
+  for (int t = 1; t < WRR; ++t)
+    if (t == i) v = a[t];
+  return v;
+}
+
+// One Jacobi round R (0..14) of the circle pairing of 16 columns.
+template <int R>
+__device__ __forceinline__ void warp_jacobi_round(double (&col)[WRR], int j, bool isv) {
+  constexpr int N1 = WRR - 1;
+  const unsigned full = 0xffffffffu;
+  const int q = (j == N1) ? R : (j == R ? N1 : (2 * R - j + 2 * N1) % N1);
+  const int a = min(j, q);
+  // rotation of the pair (a, b), formed by the A-lane of column a
+  const double djj = sel16(col, j);
+  const double dqq = __shfl_sync(full, djj, q);
+  const double ajq = sel16(col, q);
+  double c = 1.0, sn = 0.0;
+  if (!isv && j == a) {
+    const double app = djj, aqq = dqq, apq = ajq;
+    const double tiny = DBL_EPSILON * 1e-3;
+    if (fabs(apq) > 1e-300 && apq * apq > tiny * tiny * fabs(app * aqq)) {
+      const float d = static_cast<float>(aqq - app), h = static_cast<float>(2.0 * apq);
+      const float tf = (d >= 0.0f ? h : -h) / (fabsf(d) + sqrtf(fmaf(d, d, h * h)));
+      const float cf = rsqrtf(fmaf(tf, tf, 1.0f));
+      c = static_cast<double>(cf);
+      sn = static_cast<double>(tf) * static_cast<double>(cf);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const double f = fma(-0.5, fma(c, c, sn * sn), 1.5);
+        c *= f;
+        sn *= f;
+      }
+    }
+  }
+  // column rotation of this lane's pair: new a = c a - s b ; new b = s a + c b
+  const double cp = __shfl_sync(full, c, a);
+  const double sp = __shfl_sync(full, sn, a);
+  const int partner = (isv ? WRR : 0) + q;
+#pragma unroll
+  for (int i = 0; i < WRR; ++i) {
+    const double o = __shfl_sync(full, col[i], partner);
+    col[i] = (j == a) ? fma(cp, col[i], -sp * o) : fma(sp, o, cp * col[i]);
+  }
+  // row rotations of all 8 pairs (A lanes only; every lane joins the shuffles)
+#pragma unroll
+  for (int p = 0; p < WRR / 2; ++p) {
+    const int pa0 = (p == 0) ? R : (R + p) % N1;
+    const int pb0 = (p == 0) ? N1 : (R - p + N1) % N1;
+    const int pa = pa0 < pb0 ? pa0 : pb0;
+    const int pb = pa0 < pb0 ? pb0 : pa0;
+    const double cc = __shfl_sync(full, c, pa);
+    const double ss = __shfl_sync(full, sn, pa);
+    if (!isv) {
+      const double x = col[pa], y = col[pb];
+      col[pa] = fma(cc, x, -ss * y);
+      col[pb] = fma(ss, x, cc * y);
+    }
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void warp_jacobi_rounds(double (&col)[WRR], int j, bool isv) {
+  if constexpr (R < WRR - 1) {
+    warp_jacobi_round<R>(col, j, isv);
+    warp_jacobi_rounds<R + 1>(col, j, isv);
+  }
+}
+
+// sh: 2 * 16 * 16 doubles of shared memory; Z (ldz) and theta_out in shared memory.
+__device__ bool warp_rr_general(const double* gb, const double* ga, int P, const int* idx, int s, int nsel,
+                                int largest, double chol_tol, double* Z, int ldz, double* sh, double* theta_out) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int j = lane & (WRR - 1);
+  const bool isv = lane >= WRR;
+  const bool live = j < s;
+  // D scaling from diag(B)
+  double dj = 0.0;
+  int bad = 0;
+  if (!isv && live) {
+    const double d = gb[idx[j] * P + idx[j]];
+    bad = (!(d > 0.0) || !isfinite(d)) ? 1 : 0;
+    dj = d > 0.0 ? 1.0 / sqrt(d) : 0.0;
+  }
+  if (__any_sync(full, bad)) return false;
+  double colB[WRR], col[WRR];
+#pragma unroll
+  for (int i = 0; i < WRR; ++i) {
+    const double di = __shfl_sync(full, dj, i);
+    if (!isv && live && i < s) {
+      const double f = di * dj;
+      colB[i] = gb[idx[i] * P + idx[j]] * f;
+      col[i] = ga[idx[i] * P + idx[j]] * f;
+    } else {
+      colB[i] = (!isv && i == j) ? 1.0 : 0.0;
+      col[i] = 0.0;
+    }
+  }
+  // Cholesky B = L L^T (lanes 0..15; the V lanes follow the shuffles)
+  int fail = 0;
+#pragma unroll
+  for (int k = 0; k < WRR; ++k) {
+    const double pk = __shfl_sync(full, colB[k], k);
+    if (k < s && !(pk > chol_tol)) fail = 1;
+    const double piv = sqrt(fmax(pk, 1e-300));
+    const double inv = 1.0 / piv;
+    if (j == k && !isv) {
+      colB[k] = piv;
+#pragma unroll
+      for (int i = k + 1; i < WRR; ++i) colB[i] *= inv;
+    }
+    double lk[WRR];
+#pragma unroll
+    for (int i = k + 1; i < WRR; ++i) lk[i] = __shfl_sync(full, colB[i], k);
+    double ljk = 0.0;
+#pragma unroll
+    for (int i = k + 1; i < WRR; ++i)
+      if (i == j) ljk = lk[i];
+    if (!isv && j > k) {
+#pragma unroll
+      for (int i = k + 1; i < WRR; ++i) colB[i] = fma(-lk[i], ljk, colB[i]);
+    }
+  }
+  if (fail) return false;
+  double* Ls = sh;              // L, row-major 16 x 16 (lower part)
+  double* Ts = sh + WRR * WRR;  // transpose staging
+  if (!isv) {
+#pragma unroll
+    for (int i = 0; i < WRR; ++i) Ls[i * WRR + j] = (i >= j) ? colB[i] : 0.0;
+  }
+  __syncwarp();
+  // Y = L^-1 A (column j), then C = L^-1 Y^T
+#pragma unroll
+  for (int pass = 0; pass < 2; ++pass) {
+    if (!isv) {
+      double y[WRR];
+#pragma unroll
+      for (int i = 0; i < WRR; ++i) {
+        double v = col[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) v = fma(-Ls[i * WRR + k], y[k], v);
+        y[i] = v / Ls[i * WRR + i];
+      }
+#pragma unroll
+      for (int i = 0; i < WRR; ++i) Ts[i * WRR + j] = y[i];
+    }
+    __syncwarp();
+    if (!isv) {
+#pragma unroll
+      for (int i = 0; i < WRR; ++i) col[i] = Ts[j * WRR + i];  // column j of Y^T = row j of Y
+    }
+    __syncwarp();
+  }
+  // symmetrise C (col holds row j of C)
+  if (!isv) {
+#pragma unroll
+    for (int i = 0; i < WRR; ++i) Ts[i * WRR + j] = col[i];
+  }
+  __syncwarp();
+  if (!isv) {
+#pragma unroll
+    for (int i = 0; i < WRR; ++i) col[i] = 0.5 * (col[i] + Ts[j * WRR + i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < WRR; ++i) col[i] = (i == j) ? 1.0 : 0.0;  // V = I
+  }
+  __syncwarp();
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    if (!isv) {
+#pragma unroll
+      for (int i = 0; i < WRR; ++i) {
+        const double v = col[i] * col[i];
+        if (i == j) dia += v; else off += v;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      off += __shfl_xor_sync(full, off, o);
+      dia += __shfl_xor_sync(full, dia, o);
+    }
+    if (!(off > jacobi_stop2(s) * dia)) break;
+    warp_jacobi_rounds<0>(col, j, isv);
+  }
+  // eigenvalues (the diagonal) ranked among the live columns
+  const double lam = isv ? 0.0 : sel16(col, j);
+  int rank = 0;
+#pragma unroll
+  for (int i = 0; i < WRR; ++i) {
+    const double li = __shfl_sync(full, lam, i);
+    if (i < s && live && !isv) {
+      const bool before = largest ? (li > lam || (li == lam && i < j)) : (li < lam || (li == lam && i < j));
+      if (before) ++rank;
+    }
+  }
+  int* ord = reinterpret_cast<int*>(Ts);
+  if (!isv && live && rank < nsel) {
+    ord[rank] = j;
+    theta_out[rank] = lam;
+  }
+  __syncwarp();
+  // Z[:, q] = D L^-T V[:, ord[q]]: lane q < nsel takes column ord[q] from the V lanes
+  const int src = WRR + ((lane < nsel) ? ord[lane] : 0);
+  double v[WRR], dall[WRR];
+#pragma unroll
+  for (int i = 0; i < WRR; ++i) {
+    v[i] = __shfl_sync(full, col[i], src);
+    dall[i] = __shfl_sync(full, dj, i);
+  }
+  if (lane < nsel) {
+    double z[WRR];
+#pragma unroll
+    for (int i = WRR - 1; i >= 0; --i) {
+      double t = v[i];
+#pragma unroll
+      for (int k = i + 1; k < WRR; ++k) t = fma(-Ls[k * WRR + i], z[k], t);
+      z[i] = t / Ls[i * WRR + i];
+    }
+#pragma unroll
+    for (int i = 0; i < WRR; ++i)
+      if (i < s) Z[i * ldz + lane] = z[i] * dall[i];
+  }
+  __syncwarp();
+  return true;
+}
+
+// Rayleigh-Ritz of the small step: the register-resident warp version when
+// the CTA is a single warp and the problem has at most 16 columns.
+template <int NT>
+__device__ bool rr_general(const double* gb, const double* ga, int P, const int* idx, int s, int nsel, int largest,
+                           double chol_tol, SmallSmem sm, double* dsc, double* theta_out, double* red, double* rc,
+                           double* rs, int* ra, int* rb, int* order, int* sflag) {
+  if constexpr (NT == 32) {
+    if (s <= WRR) return warp_rr_general(gb, ga, P, idx, s, nsel, largest, chol_tol, sm.Z, sm.ld, sm.T, theta_out);
+  }
+  return cta_rr_general(gb, ga, P, idx, s, nsel, largest, chol_tol, sm, dsc, theta_out, red, rc, rs, ra, rb, order,
+                        sflag);
+}
+
 // `ctrl` points to the CTA's shared-memory copy of the control block.
+template <int NT>
 __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns, int mode,
                                 double* smem) {
   __shared__ double red[ST_WIDE / 32];
@@ -517,7 +795,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
   if (mode == SM_INIT) {
     for (int i = threadIdx.x; i < m; i += blockDim.x) idx[i] = i;
     __syncthreads();
-    const bool ok = cta_rr_general(gb, ga, P, idx, m, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc,
+    const bool ok = rr_general<NT>(gb, ga, P, idx, m, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc,
                                    rs, ra, rb, order, &sflag);
     if (threadIdx.x == 0) {
       ctrl->iter = 0;
@@ -642,12 +920,12 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
         if (ctrl->active[c]) idx[m + na + q++] = 2 * m + c;
     }
     __syncthreads();
-    ok = cta_rr_general(gb, ga, P, idx, m + 2 * na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs,
+    ok = rr_general<NT>(gb, ga, P, idx, m + 2 * na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs,
                         ra, rb, order, &sflag);
     if (!ok) withp = 0;
   }
   if (!ok) {
-    ok = cta_rr_general(gb, ga, P, idx, m + na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs, ra,
+    ok = rr_general<NT>(gb, ga, P, idx, m + na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs, ra,
                         rb, order, &sflag);
   }
   if (!ok) {
@@ -695,7 +973,7 @@ __global__ void __launch_bounds__(NT) k_small_step(LobpcgCtrl* ctrl, const doubl
   const double* src = reinterpret_cast<const double*>(ctrl);
   for (int i = threadIdx.x; i < W; i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  small_step_body(&sctrl, gram, ns, mode, smem);
+  small_step_body<NT>(&sctrl, gram, ns, mode, smem);
   __syncthreads();
   double* back = reinterpret_cast<double*>(ctrl);
   for (int i = threadIdx.x; i < W; i += blockDim.x) back[i] = dst[i];
@@ -740,6 +1018,14 @@ __global__ void __launch_bounds__(ST) k_small_dense(const double* __restrict__ a
 
 }  // namespace
 
+// SPECTRAL_INIT_SMALL_STEP=cta keeps the multi-warp small step for every
+// width (the single-warp version is the default up to 16 columns); read on
+// every call, so one process can compare both.
+bool small_step_cta_forced() {
+  const char* e = std::getenv("SPECTRAL_INIT_SMALL_STEP");
+  return e != nullptr && std::string(e) == "cta";
+}
+
 void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode, int m) {
   const int LDS = 3 * MAXM;
   const size_t smem = sizeof(double) * 5 * LDS * LDS;
@@ -749,13 +1035,18 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
                                  static_cast<int>(smem)));
     SI_CUDA(cudaFuncSetAttribute(k_small_step<ST_WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
+    SI_CUDA(cudaFuncSetAttribute(k_small_step<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
     attr_set[ex.device] = true;
   }
-  // the Rayleigh-Ritz problem has up to ns * m rows: wide blocks get more threads
+  // the Rayleigh-Ritz problem has up to ns * m rows: up to 16 fit one warp's
+  // registers; wider blocks get a CTA, the widest the most threads
   if (ns * m > 24)
     k_small_step<ST_WIDE><<<1, ST_WIDE, smem, ex.stream>>>(ctrl, gram, ns, mode);
-  else
+  else if (ns * m > WRR || small_step_cta_forced())
     k_small_step<ST><<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  else
+    k_small_step<32><<<1, 32, smem, ex.stream>>>(ctrl, gram, ns, mode);
   SI_LAUNCH_CHECK();
 }
 
