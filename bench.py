@@ -52,7 +52,16 @@ def parse_args():
     p.add_argument("--background", type=float, default=0.05)
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--spmm-reps", type=int, default=40)
-    p.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU LOBPCG per baseline sample")
+    p.add_argument("--tol", type=float, default=1e-7,
+                   help="LOBPCG tolerance of the mixed / learned legs (the headline): tight enough that their "
+                        "subspace is within 1e-4 of the FP64 oracle on this graph; the plain FP64 leg runs at "
+                        "the crate's 1e-5 (the drop-in)")
+    p.add_argument("--no-oracle", action="store_true", help="skip the CPU ARPACK accuracy oracle")
+    p.add_argument("--accuracy-sweep", action="store_true",
+                   help="one JSON line: mixed/learned/FP64 solves at several tolerances, time and error vs the oracle")
+    p.add_argument("--cpu-threads", type=int, default=0, help="threads of the CPU baseline (0: all)")
+    p.add_argument("--cpu-only", action="store_true",
+                   help="only the CPU baseline (one converged solve per step), for the 1-thread measurement")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
@@ -292,14 +301,21 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         if WEIGHTS_PATH.exists():
             model = WarmStartModel.load(ctx=ctx)
             model.attach()
-    legs = [(0, 0, "fp64"), (1, 0, "mixed")] + ([(1, 1, "learned")] if model is not None else [])
-    head = legs[-1][2]
+    # (name, precision, warm start, tol): the plain FP64 solve at the crate's
+    # tolerance is the drop-in; the mixed / learned legs run at --tol
+    legs = [("fp64", 0, 0, 0.0), ("mixed", 1, 0, a.tol)]
+    if model is not None:
+        legs.append(("learned", 1, 1, a.tol))
+    if a.tol < 1e-5:
+        legs.append(("fp64_same_tol", 0, 0, a.tol))
+    head = "learned" if model is not None else "mixed"
 
-    def solve(precision: int, warm: int = 0):
+    def solve(precision: int, warm: int = 0, tol: float = 0.0):
         cfg = SiConfig()
         lib.si_config_default(C.byref(cfg))
         cfg.precision = precision
         cfg.warm_start = warm
+        cfg.tol = tol
         vals = (C.c_double * k)()
         vecs = torch.empty(n, k, dtype=torch.float64, device=dev)
         level = C.c_int32(-1)
@@ -316,20 +332,43 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
 
     if a.profile_solve:
         out = {}
-        for prec, warm, name in legs:
-            solve(prec, warm)
-            ms, vals, _, level, rep = solve(prec, warm)
+        for name, prec, warm, tol in legs:
+            solve(prec, warm, tol)
+            ms, vals, _, level, rep = solve(prec, warm, tol)
             out[name] = {"ms": ms, "iterations": rep.iterations, "level": level, "max_residual": rep.max_residual,
                          "learned_start": rep.learned_start}
         print(json.dumps({"profile_solve": True, "n": n, "nnz": nnz, **out}))
         return
 
+    oracle = None
+    if rank == 0 and world == 1 and not a.no_oracle:
+        oracle = host_oracle(a, indptr, indices, data, k)
+
+    if a.accuracy_sweep:
+        rows = []
+        for name, prec, warm in (("mixed", 1, 0), ("learned", 1, 1), ("fp64", 0, 0)):
+            if warm and model is None:
+                continue
+            for tol in (1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8):
+                solve(prec, warm, tol)
+                ms, vals, vecs, level, rep = solve(prec, warm, tol)
+                r = {"leg": name, "tol": tol, "ms": ms, "iterations": rep.iterations,
+                     "fp32_iterations": rep.fp32_iterations, "max_residual": rep.max_residual,
+                     "learned_start": rep.learned_start}
+                if oracle is not None:
+                    r["vs_oracle"] = oracle_errors(oracle, vals, vecs)
+                rows.append(r)
+                print(json.dumps(r), flush=True)
+        print(json.dumps({"accuracy_sweep": True, "n": n, "nnz": nnz, "rows": rows,
+                          "oracle": None if oracle is None else oracle["summary"]}))
+        return
+
     results = {}
     clocks = None
     launches_per_step = None
-    for prec, warm, name in legs:
+    for name, prec, warm, tol in legs:
         for _ in range(a.warmup):
-            solve(prec, warm)
+            solve(prec, warm, tol)
         barrier()
         torch.cuda.synchronize()
         sampler = ClockSampler(local) if name == head else None
@@ -338,7 +377,7 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         l0 = lib.si_kernel_launches()
         times, last = [], None
         for _ in range(a.steps):
-            ms, vals, vecs, level, rep = solve(prec, warm)
+            ms, vals, vecs, level, rep = solve(prec, warm, tol)
             times.append(ms)
             last = (vals, vecs, level, rep)
         torch.cuda.synchronize()
@@ -348,12 +387,14 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
             launches_per_step = (lib.si_kernel_launches() - l0) / a.steps
         ms_mean = max_over_ranks(statistics.mean(times))
         vals, vecs, level, rep = last
-        results[name] = {"ms": ms_mean, "ms_all": times, "eigenvalues": vals, "level": level,
-                         "iterations": rep.iterations, "fp32_iterations": rep.fp32_iterations,
+        results[name] = {"ms": ms_mean, "ms_all": times, "tol": tol if tol > 0 else 1e-5, "eigenvalues": vals,
+                         "level": level, "iterations": rep.iterations, "fp32_iterations": rep.fp32_iterations,
                          "restarts": rep.restarts, "max_residual": rep.max_residual,
                          "learned_start": rep.learned_start, "vecs": vecs}
+        if oracle is not None:
+            results[name]["vs_oracle"] = oracle_errors(oracle, vals, vecs)
 
-    # agreement of the two solves: largest principal-angle sine and eigenvalue differences
+    # agreement of the headline solve with the plain FP64 solve: largest principal-angle sine, eigenvalues
     qa, _ = torch.linalg.qr(results["fp64"]["vecs"])
     qb, _ = torch.linalg.qr(results[head]["vecs"])
     sin_theta = float(torch.linalg.matrix_norm(qb - qa @ (qa.T @ qb), ord=2))
@@ -376,6 +417,7 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         lib.si_config_default(C.byref(cfg))
         cfg.precision = 1
         cfg.warm_start = 1 if head == "learned" else 0
+        cfg.tol = a.tol
         rep = SiReport()
 
         def call():
@@ -398,7 +440,7 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
     # ---- CPU baseline (rank 0, N=1) ---------------------------------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline_sample(a, indptr, indices, v64, sq, budget=a.cpu_budget)
+        cpu = cpu_baseline_sample(a, indptr, indices, data)
 
     peaks, peak_src = load_peaks()
     hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
@@ -412,6 +454,10 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
     if rank != 0:
         return
     value_s = results[head]["ms"] / 1e3
+
+    def leg(name):
+        return {k2: v for k2, v in results[name].items() if k2 != "vecs"}
+
     line = {
         "metric": METRIC,
         "value": value_s,
@@ -430,18 +476,21 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
                    f"{(nnz * 12 + (n + 1) * 8) / 1e6:.0f} MB f64 / {(nnz * 8 + (n + 1) * 8) / 1e6:.0f} MB f32)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "graph_build_s": round(t_gen, 2),
+                   "tol_value_leg": a.tol, "tol_fp64_leg": 1e-5,
                    "warm_start": ("learned (committed network weights, trained on the n=10k-200k family)"
                                   if head == "learned" else "random (no network weights found)")},
-        "fp64": {k2: v for k2, v in results["fp64"].items() if k2 != "vecs"},
-        "mixed": {k2: v for k2, v in results["mixed"].items() if k2 != "vecs"},
-        **({"learned": {k2: v for k2, v in results["learned"].items() if k2 != "vecs"}} if head == "learned" else {}),
+        **{name: leg(name) for name in results},
         "speedup_mixed_vs_fp64": results["fp64"]["ms"] / results["mixed"]["ms"],
         "speedup_value_vs_fp64": results["fp64"]["ms"] / results[head]["ms"],
+        **({"speedup_value_vs_fp64_same_tol": results["fp64_same_tol"]["ms"] / results[head]["ms"]}
+           if "fp64_same_tol" in results else {}),
         "value_vs_fp64": {"leg": head, "sin_theta_max": sin_theta, "eigenvalue_rel_diff_max": ev_rel},
+        "value_vs_oracle": (None if oracle is None else
+                            {"leg": head, **results[head]["vs_oracle"], "oracle": oracle["summary"]}),
         "spmm": {"ms_f64": ms64, "ms_f32": ms32, "gbs_f64": gbs64, "gbs_f32": gbs32,
                  "algorithmic_bytes_f64": bytes64, "algorithmic_bytes_f32": bytes32,
                  "bytes_formula": "nnz*(4 idx + s_val) + (n+1)*8 indptr + 2*n*4*s_x (x read, y written; 4 columns)"},
-        "roofline": {"bound": "hbm", "kernel": "k_spmm_vec<float,float,4,*> (f32 SpMM, 4 columns)",
+        "roofline": {"bound": "hbm", "kernel": "f32 SpMM, 4 columns (the autotuned kernel; ncu summary in profiles/)",
                      "achieved": gbs32, "peak": hbm, "unit": "GB/s", "frac": gbs32 / hbm,
                      "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
                      else "fallback 6.65 TB/s", "traffic": traffic},
@@ -453,71 +502,109 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
     print(json.dumps(line))
 
 
-def cpu_baseline_sample(a, indptr, indices, v64, sq, budget: float):
-    """The restated CPU path on this host (OpenMP SpMM + numpy LOBPCG), bounded."""
+def host_oracle(a, indptr, indices, data, k):
+    """The FP64 accuracy oracle on the host: the crate's Laplacian built on the
+    CPU from the graph, ARPACK to machine precision (k + 6 pairs), residuals
+    and the Davis-Kahan certificate."""
     import numpy as np
+    from oracle import certified as CERT
     from oracle import cpu_baseline as CB
-    ip = indptr.cpu().numpy().astype(np.uint64)
-    ix = indices.cpu().numpy().astype(np.uint32)
-    vv = v64.cpu().numpy()
-    sqh = sq.cpu().numpy()
-    op = CB.CpuOperator(ip, ix, vv, a.n, diag=1.0)
+    t0 = time.time()
+    op, _ = CB.laplacian_operator(indptr.cpu().numpy(), indices.cpu().numpy(), data.cpu().numpy(), a.n)
+    ref = CERT.reference_eigenpairs_operator(op.apply, a.n, k, extra=6)
+    secs = time.time() - t0
+    gap = CERT.gap_after(ref, k)
+    summary = {"method": ref.method, "seconds": round(secs, 1), "eigenvalues": [float(v) for v in ref.vals],
+               "max_residual": float(np.max(ref.residuals)), "gap_k": gap,
+               "sin_theta_bound": float(np.max(ref.residuals[:k]) / gap)}
+    return {"ref": ref, "summary": summary}
+
+
+def oracle_errors(oracle, vals, vecs):
+    from oracle import certified as CERT
+    c = CERT.compare(vals, vecs.cpu().numpy(), oracle["ref"])
+    return {"sin_theta": c["sin_theta_max"], "sin_theta_subspace": c["sin_theta_subspace"],
+            "eig_rel_max": c["eig_rel_max"], "eig_abs0": c["eig_abs0"]}
+
+
+def cpu_baseline_sample(a, indptr, indices, data):
+    """The restated CPU path on this host (OpenMP C SpMM + numpy LOBPCG), one
+    solve run to completion and timed (the crate's Laplacian is built on the CPU
+    first, outside the timed solve)."""
+    from oracle import cpu_baseline as CB
+    if a.cpu_threads > 0:
+        CB.set_threads(a.cpu_threads)
+    op, sqh = CB.laplacian_operator(indptr.cpu().numpy(), indices.cpu().numpy(), data.cpu().numpy(), a.n)
     spmm_s = CB.time_spmm(op, a.nc + 1, reps=3)
-    res = CB.solve_timed(op, a.nc, a.seed, sqh, budget_s=budget)
-    nnz = len(ix)
+    res = CB.solve_measured(op, a.nc, a.seed, sqh)
+    nnz = len(op.indices)
     bytes_k3 = nnz * 12 + (a.n + 1) * 8 + 2 * a.n * (a.nc + 1) * 8
     return {"value": res["seconds"], "unit": "s", "cores": CB.threads(), "kind": "port",
-            "sample": (f"crate Level-1 solve restated on the CPU (f64, block of {a.nc + 1}, Chebyshev filter + "
-                       f"LOBPCG), run for {res['iterations']} iterations / {budget:.0f} s budget; "
-                       + ("converged" if res["converged"] else
-                          f"time to residual 1e-5 projected from the residual decay ({res['projected']})")),
-            "iterations": res["iterations"], "iterations_total": res.get("iterations_total"),
-            "per_iteration_s": res["per_iteration_s"], "filter_s": res["filter_s"],
+            "host": host_cpu(),
+            "sample": (f"one complete crate Level-1 solve restated on the CPU (f64, block of {a.nc + 1}: random start, "
+                       f"Chebyshev filter, LOBPCG with warm restarts, Rayleigh-Ritz, residual gate), measured to "
+                       f"{'convergence' if res['converged'] else 'its end (not converged)'}: "
+                       f"{res['iterations']} iterations, max residual {res['max_residual']:.2e}"),
+            "iterations": res["iterations"], "restarts": res["restarts"], "converged": res["converged"],
             "spmm_s_k3": spmm_s, "spmm_gbs_k3": bytes_k3 / spmm_s / 1e9}
+
+
+def host_cpu():
+    try:
+        model = next((ln.split(":", 1)[1].strip() for ln in Path("/proc/cpuinfo").read_text().splitlines()
+                      if ln.startswith("model name")), "unknown")
+    except OSError:
+        model = "unknown"
+    return {"nproc": os.cpu_count(), "model": model}
 
 
 def run_reference(a):
     """The reference arm: the restated CPU path on this host for the same
-    workload, metric and unit (rank 0 only)."""
+    workload, metric and unit (rank 0 only).  Each timed step is one complete
+    Level-1 solve (random start, Chebyshev filter, LOBPCG with warm restarts,
+    Rayleigh-Ritz, residual gate) on the crate's Laplacian built on the CPU;
+    the warm-up steps run the same code for one second each."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import numpy as np
     import torch
     from oracle import cpu_baseline as CB
-    from oracle import spectral_oracle as O
+    if a.cpu_threads > 0:
+        CB.set_threads(a.cpu_threads)
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     indptr, indices, data = make_graph(a, dev, 0)
-    ip = indptr.cpu().numpy().astype(np.uint64)
-    ix = indices.cpu().numpy().astype(np.uint32)
-    w = data.cpu().numpy()
     n = a.n
-    # degrees (f32 column scatter) and Laplacian values on the host, as the crate does
-    deg = np.zeros(n, dtype=np.float32)
-    CB.load().column_sum_f32(len(ix), ix.ctypes.data, w.ctypes.data, deg.ctypes.data)
-    sqh = np.sqrt(deg.astype(np.float64))
-    inv = O.inv_sqrt(sqh)
-    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(ip.astype(np.int64)))
-    vv = np.where(rows == ix, 0.0, (-inv[rows]) * w.astype(np.float64) * inv[ix.astype(np.int64)])
-    op = CB.CpuOperator(ip, ix, vv, n, diag=1.0)
+    op, sqh = CB.laplacian_operator(indptr.cpu().numpy(), indices.cpu().numpy(), data.cpu().numpy(), n)
     for _ in range(a.warmup):
         CB.solve_timed(op, a.nc, a.seed, sqh, budget_s=1.0)
-    samples = [CB.solve_timed(op, a.nc, a.seed, sqh, budget_s=a.cpu_budget) for _ in range(a.steps)]
+    samples = [CB.solve_measured(op, a.nc, a.seed, sqh) for _ in range(a.steps)]
     val = statistics.mean(s["seconds"] for s in samples)
     s0 = samples[-1]
-    cpu = {"value": val, "unit": "s", "cores": CB.threads(), "kind": "port",
-           "sample": (f"crate Level-1 solve restated on the CPU per step: Chebyshev filter + LOBPCG for "
-                      f"{a.cpu_budget:.0f} s ({s0['iterations']} iterations), time to residual 1e-5 "
-                      + ("measured" if s0["converged"] else f"projected ({s0['projected']})")),
-           "per_iteration_s": s0["per_iteration_s"], "iterations_total": s0.get("iterations_total")}
+    conv = all(x["converged"] for x in samples)
+    cpu = {"value": val, "unit": "s", "cores": CB.threads(), "kind": "port", "host": host_cpu(),
+           "sample": (f"per step one complete crate Level-1 solve restated on the CPU (f64, block of {a.nc + 1}), "
+                      f"measured to {'convergence' if conv else 'its end'}: "
+                      f"{s0['iterations']} iterations, max residual {s0['max_residual']:.2e}"),
+           "iterations": s0["iterations"], "restarts": s0["restarts"], "converged": conv,
+           "seconds_all": [x["seconds"] for x in samples]}
     line = {"metric": METRIC, "value": val, "unit": "s", "higher_is_better": False, "impl": "reference",
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": val * 1e3, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Gaussian-mixture fuzzy-kNN graph)",
-            "config": {"workload": workload_name(a), "n": n, "nnz": int(len(ix))},
+            "config": {"workload": workload_name(a), "n": n, "nnz": int(len(op.indices))},
             "cpu_baseline": cpu,
             "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def run_cpu_only(a):
+    """One JSON line: the CPU baseline alone (--steps complete solves at
+    --cpu-threads threads), for the single-thread measurement."""
+    import torch
+    indptr, indices, data = make_graph(a, torch.device("cuda", 0), 0)
+    rows = [cpu_baseline_sample(a, indptr, indices, data) for _ in range(max(1, a.steps))]
+    print(json.dumps({"cpu_only": True, "workload": workload_name(a), "threads": rows[0]["cores"],
+                      "value": statistics.mean(r["value"] for r in rows), "unit": "s", "samples": rows}))
 
 
 def run_components(a):
@@ -704,6 +791,9 @@ def run_dense(a):
 
 def main():
     a = parse_args()
+    if a.cpu_only:
+        run_cpu_only(a)
+        return
     if a.components and a.impl == "ours":
         run_components(a)
         return
