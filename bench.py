@@ -685,11 +685,12 @@ def run_configs(a):
         model = WarmStartModel.load(ctx=ctx)
         model.attach()
 
-    def solve(lap, nc, prec=0, warm=0, level=-1, over=-1, nbiter=0):
+    def solve(lap, nc, prec=0, warm=0, level=-1, over=-1, nbiter=0, tol=0.0):
         cfg = SiConfig()
         lib.si_config_default(C.byref(cfg))
         cfg.precision, cfg.warm_start, cfg.force_level = prec, warm, level
         cfg.rsvd_oversampling, cfg.rsvd_nbiter = over, nbiter
+        cfg.tol = tol
         k = nc + 1
         vals = (C.c_double * k)()
         vecs = torch.empty(lap.n, k, dtype=torch.float64, device=dev)
@@ -723,28 +724,69 @@ def run_configs(a):
     g = synthetic.fuzzy_graph_gpu(idx, dist, sigma, rho)
     del idx, dist
     lap = DeviceLaplacian((g[0], g[1], g[2], n), ctx=ctx)
+    import argparse as _ap
+    orc = None if a.no_oracle else host_oracle(_ap.Namespace(n=n), g[0], g[1], g[2], 3)
     r64, v64, x64 = solve(lap, 2)
+    if orc is not None:
+        r64["vs_oracle"] = oracle_errors(orc, v64, x64)
     line = {"config": "n=200k: 30 anisotropic clusters (Dirichlet 0.5 sizes) in 50-D + 2% background, k=15, "
-                      "n_components=2", "nnz": lap.nnz, "fp64": r64}
-    for name, prec, warm in (("mixed", 1, 0), ("learned", 1, 1)):
+                      "n_components=2", "nnz": lap.nnz, "fp64": r64,
+            "oracle": None if orc is None else orc["summary"]}
+    legs = [("mixed", 1, 0, 0.0), ("learned", 1, 1, 0.0), ("fp64_tol", 0, 0, a.tol), ("mixed_tol", 1, 0, a.tol),
+            ("learned_tol", 1, 1, a.tol)]
+    for name, prec, warm, tol in legs:
         if warm and model is None:
             continue
-        r, v, xv = solve(lap, 2, prec, warm)
+        r, v, xv = solve(lap, 2, prec, warm, tol=tol)
+        r["tol"] = tol if tol > 0 else 1e-5
         r["eigenvalue_abs_diff_vs_fp64"] = float(np.max(np.abs(v - v64)))
         r["sin_theta_vs_fp64"] = sin_theta(xv[:, 1:], x64[:, 1:])
         r["speedup_vs_fp64"] = r64["ms"] / r["ms"]
+        if orc is not None:
+            r["vs_oracle"] = oracle_errors(orc, v, xv)
         line[name] = r
     line["eigengap_2_3"] = float(v64[2] - v64[1])
     print(json.dumps(line), flush=True)
     del lap, g
 
-    # n = 1M benchmark graph: n_components = 8, and the rSVD path (oversampling 10, 4 power iterations)
-    ip, ix, dv = make_graph(a, dev, 0)
-    lap = DeviceLaplacian((ip, ix, dv, a.n), ctx=ctx)
-    line = {"config": workload_name(a).replace(f"n_components={a.nc}", "n_components=8 and rSVD"), "nnz": lap.nnz}
-    line["lobpcg_nc8_fp64"], _, _ = solve(lap, 8)
-    line["lobpcg_nc8_mixed"], _, _ = solve(lap, 8, 1)
+    # n = 1M, k = 30 (the large-graph configuration: 100-cluster mixture in 50-D + 5 % background, ~45M
+    # stored entries): LOBPCG at n_components 2 and 8 (FP64 at the crate's tolerance, mixed at --tol), the
+    # rSVD path (oversampling 10, 4 power iterations), and the SpMM bandwidth at 4- and 16-wide blocks
+    import argparse as _ap
+    a30 = _ap.Namespace(**vars(a))
+    a30.k = 30
+    ip, ix, dv = make_graph(a30, dev, 0)
+    lap = DeviceLaplacian((ip, ix, dv, a30.n), ctx=ctx)
+    line = {"config": workload_name(a30).replace(f"n_components={a.nc}", "n_components 2 and 8, LOBPCG and rSVD"),
+            "nnz": lap.nnz}
+    op = lap.op()
+    peaks, peak_src = load_peaks()
+    hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+    for ld in (4, 16):
+        for f32 in (True, False):
+            xb = 4 if f32 else 8
+            x = torch.randn(a30.n, ld, dtype=torch.float32 if f32 else torch.float64, device=dev)
+            y = torch.empty_like(x)
+            fn = lib.si_spmm_f32 if f32 else lib.si_spmm
+            for _ in range(3):
+                ctx.check(fn(ctx.ptr, C.byref(op), x.data_ptr(), y.data_ptr(), ld))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(20):
+                ctx.check(fn(ctx.ptr, C.byref(op), x.data_ptr(), y.data_ptr(), ld))
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / 20
+            byt = lap.nnz * (4 + xb) + (a30.n + 1) * 8 + 2 * a30.n * ld * xb
+            line[f"spmm_ld{ld}_{'f32' if f32 else 'f64'}"] = {"ms": ms, "gbs": byt / ms / 1e6,
+                                                              "frac_of_hbm": byt / ms / 1e6 / hbm}
+            del x, y
+    line["hbm_peak_gbs"] = {"value": hbm, "source": peak_src}
     for nc in (2, 8):
+        line[f"lobpcg_nc{nc}_fp64"], _, _ = solve(lap, nc)
+        line[f"lobpcg_nc{nc}_mixed"], _, _ = solve(lap, nc, 1, tol=a.tol)
         line[f"rsvd_nc{nc}"], _, _ = solve(lap, nc, 0, 0, 4, 10, 4)
     print(json.dumps(line), flush=True)
 
