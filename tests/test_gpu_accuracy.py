@@ -143,22 +143,32 @@ def test_config1_connected_default_tolerance_bound(gpu_ctx):
 def test_config1_pipeline_matches_oracle(gpu_ctx):
     """spectral_init on the 8-component graph with its points: the crate routes
     to embed_disconnected with the spectral meta-embedding (src/lib.rs:217-229,
-    src/multi_component.rs:16-312).  Per component the embedding matches the
-    oracle's pre-noise one up to sign (each component is solved densely), and
-    the component centres match up to per-axis sign."""
+    src/multi_component.rs:16-312).  The meta-embedding gives several of these
+    components a range of (nearly) zero, so after the final scale to 10 their
+    points sit within the 1e-4 noise of one position: those are checked for
+    position and spread; components with a visible spread (> 1e-2) are
+    compared with the oracle's pre-noise embedding up to sign (each component
+    is solved densely, its eigenvalues are 0.01-0.03 apart)."""
     import spectral_init_b200 as si
     x, g, _, _ = _config1(5.0)
     out = si.spectral_init(g, 2, 42, data=x, ctx=gpu_ctx).astype(np.float64)
     pre = O.scale_coords(O.spectral_init_prenoise(g, 2, 42, data=x), 10.0).astype(np.float64)
     labels, nc = O.find_components_fast(g)
+    spread_seen = 0
     for c in range(nc):
         idx = np.nonzero(labels == c)[0]
+        assert np.allclose(np.abs(out[idx].mean(0)), np.abs(pre[idx].mean(0)), atol=5e-2), c
+        spread = float(pre[idx].std(0).min())
+        if spread < 1e-2:
+            assert float(out[idx].std(0).max()) < 1e-3 + 10 * spread, c
+            continue
+        spread_seen += 1
         for ax in range(2):
             a = out[idx, ax] - out[idx, ax].mean()
             b = pre[idx, ax] - pre[idx, ax].mean()
             cos = abs(a @ b) / max(np.linalg.norm(a) * np.linalg.norm(b), 1e-300)
             assert cos > 0.99, (c, ax, cos)
-        assert np.allclose(np.abs(out[idx].mean(0)), np.abs(pre[idx].mean(0)), atol=5e-2)
+    assert spread_seen >= 1
 
 
 # ---- the n = 200k configuration ------------------------------------------------------------
