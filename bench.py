@@ -256,17 +256,20 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
     ctx.check(lib.si_build_laplacian(ctx.ptr, C.byref(g), inv.data_ptr(), v64.data_ptr(), v32.data_ptr()))
     op = SiOperator(n, nnz, indptr.data_ptr(), indices.data_ptr(), v64.data_ptr(), v32.data_ptr(), 1.0)
 
-    # ---- SpMM (the roofline kernel) -------------------------------------------------------
+    # ---- SpMM (the roofline kernel): the prepared operator, kernels back to back on the stream ----
+    plan = C.c_void_p()
+    ctx.check(lib.si_operator_plan_create(ctx.ptr, C.byref(op), C.byref(plan)))
+
     def time_spmm(x, y, f32: bool, reps: int):
-        fn = lib.si_spmm_f32 if f32 else lib.si_spmm
+        fn = lib.si_spmm_planned_f32 if f32 else lib.si_spmm_planned
         for _ in range(3):
-            ctx.check(fn(ctx.ptr, C.byref(op), x.data_ptr(), y.data_ptr(), 4))
+            ctx.check(fn(ctx.ptr, plan, x.data_ptr(), y.data_ptr(), 4))
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(reps):
-            ctx.check(fn(ctx.ptr, C.byref(op), x.data_ptr(), y.data_ptr(), 4))
+            ctx.check(fn(ctx.ptr, plan, x.data_ptr(), y.data_ptr(), 4))
         e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1) / reps
@@ -286,6 +289,7 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
     bytes32 = nnz * (4 + 4) + (n + 1) * 8 + 2 * n * 4 * 4
     gbs64 = bytes64 / (ms64 * 1e-3) / 1e9
     gbs32 = bytes32 / (ms32 * 1e-3) / 1e9
+    lib.si_operator_plan_destroy(plan)
     if a.spmm_profile:
         print(json.dumps({"spmm_profile": True, "n": n, "nnz": nnz, "ms_f64": ms64, "ms_f32": ms32,
                           "gbs_f64": gbs64, "gbs_f32": gbs32}))
@@ -760,6 +764,8 @@ def run_configs(a):
     line = {"config": workload_name(a30).replace(f"n_components={a.nc}", "n_components 2 and 8, LOBPCG and rSVD"),
             "nnz": lap.nnz}
     op = lap.op()
+    plan = C.c_void_p()
+    ctx.check(lib.si_operator_plan_create(ctx.ptr, C.byref(op), C.byref(plan)))
     peaks, peak_src = load_peaks()
     hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
     for ld in (4, 16):
@@ -767,15 +773,15 @@ def run_configs(a):
             xb = 4 if f32 else 8
             x = torch.randn(a30.n, ld, dtype=torch.float32 if f32 else torch.float64, device=dev)
             y = torch.empty_like(x)
-            fn = lib.si_spmm_f32 if f32 else lib.si_spmm
+            fn = lib.si_spmm_planned_f32 if f32 else lib.si_spmm_planned
             for _ in range(3):
-                ctx.check(fn(ctx.ptr, C.byref(op), x.data_ptr(), y.data_ptr(), ld))
+                ctx.check(fn(ctx.ptr, plan, x.data_ptr(), y.data_ptr(), ld))
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             e0.record(stream)
             for _ in range(20):
-                ctx.check(fn(ctx.ptr, C.byref(op), x.data_ptr(), y.data_ptr(), ld))
+                ctx.check(fn(ctx.ptr, plan, x.data_ptr(), y.data_ptr(), ld))
             e1.record(stream)
             e1.synchronize()
             ms = e0.elapsed_time(e1) / 20
@@ -783,6 +789,7 @@ def run_configs(a):
             line[f"spmm_ld{ld}_{'f32' if f32 else 'f64'}"] = {"ms": ms, "gbs": byt / ms / 1e6,
                                                               "frac_of_hbm": byt / ms / 1e6 / hbm}
             del x, y
+    lib.si_operator_plan_destroy(plan)
     line["hbm_peak_gbs"] = {"value": hbm, "source": peak_src}
     for nc in (2, 8):
         line[f"lobpcg_nc{nc}_fp64"], _, _ = solve(lap, nc)

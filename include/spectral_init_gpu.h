@@ -190,6 +190,20 @@ si_status si_spmm(si_ctx* ctx, const si_operator* op, const double* x, double* y
 /* Same with f32 blocks and op->values_f32 (accumulation in f64). */
 si_status si_spmm_f32(si_ctx* ctx, const si_operator* op, const float* x, float* y, uint32_t k);
 
+/* A device operator prepared for repeated products (the crate's CsrOperator,
+ * src/operator.rs:174-228, holds its matrix across LinearOperator::apply
+ * calls): the row partitions of the tiled / gather / panel kernels are built
+ * once, the panel kernel's x windows once per block width.  The operator's
+ * arrays must stay allocated and unchanged while the plan lives. */
+typedef struct si_operator_plan si_operator_plan;
+si_status si_operator_plan_create(si_ctx* ctx, const si_operator* op, si_operator_plan** out);
+void si_operator_plan_destroy(si_operator_plan* plan);
+/* LinearOperator::apply on a prepared operator: y = A x, blocks [n x k]
+ * (device, f64; the f32 form uses op->values_f32).  Asynchronous: queued on
+ * the context's stream (si_ctx_synchronize waits). */
+si_status si_spmm_planned(si_ctx* ctx, const si_operator_plan* plan, const double* x, double* y, uint32_t k);
+si_status si_spmm_planned_f32(si_ctx* ctx, const si_operator_plan* plan, const float* x, float* y, uint32_t k);
+
 /* solve_eigenproblem (src/solvers/mod.rs:70-224) on a device operator.
  * eigvals: HOST f64 [n_components+1]; eigvecs: DEVICE f64 [n x (n_components+1)];
  * sqrt_deg: DEVICE f64 [n] (trivial-vector hint).  *level receives 0..5. */

@@ -80,6 +80,10 @@ _SIGNATURES = {
     "si_find_components": (C.c_int, [vp, C.POINTER(SiCsrF32), vp, u64p]),
     "si_spmm": (C.c_int, [vp, C.POINTER(SiOperator), vp, vp, C.c_uint32]),
     "si_spmm_f32": (C.c_int, [vp, C.POINTER(SiOperator), vp, vp, C.c_uint32]),
+    "si_operator_plan_create": (C.c_int, [vp, C.POINTER(SiOperator), C.POINTER(vp)]),
+    "si_operator_plan_destroy": (None, [vp]),
+    "si_spmm_planned": (C.c_int, [vp, vp, vp, vp, C.c_uint32]),
+    "si_spmm_planned_f32": (C.c_int, [vp, vp, vp, vp, C.c_uint32]),
     "si_solve_eigenproblem": (C.c_int, [vp, C.POINTER(SiOperator), C.c_uint32, C.c_uint64, vp,
                                         C.POINTER(SiConfig), vp, vp, i32p, C.POINTER(SiReport)]),
     "si_solve_eigenproblem_host": (C.c_int, [vp, C.POINTER(SiCsrF64), C.c_uint32, C.c_uint64,

@@ -466,3 +466,37 @@ class CsrOperator:
         else:
             self.ctx.check(self.ctx.lib.si_spmm_f32(self.ctx.ptr, C.byref(self.c()), x.data_ptr(), y.data_ptr(), k))
         return y
+
+    # ---- prepared operator (si_operator_plan): repeated products without per-call set-up ----
+    def prepare(self) -> "CsrOperator":
+        """Build the operator's plan once (row partitions, panel windows on
+        first use of each width); ``apply_prepared`` then reuses it."""
+        if getattr(self, "_plan", None) is None:
+            h = C.c_void_p()
+            self.ctx.check(self.ctx.lib.si_operator_plan_create(self.ctx.ptr, C.byref(self.c()), C.byref(h)))
+            self._plan = h
+        return self
+
+    def apply_prepared(self, x, y=None):
+        """``y = diag * x + V x`` through the prepared operator, queued on the
+        library's stream without waiting (``ctx.synchronize()`` waits)."""
+        torch = _torch()
+        self.prepare()
+        x = x.contiguous()
+        if y is None:
+            y = torch.empty_like(x)
+        k = x.shape[1] if x.dim() == 2 else 1
+        fn = self.ctx.lib.si_spmm_planned if x.dtype == torch.float64 else self.ctx.lib.si_spmm_planned_f32
+        self.ctx.check(fn(self.ctx.ptr, self._plan, x.data_ptr(), y.data_ptr(), k))
+        return y
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None) is not None:
+            self.ctx.lib.si_operator_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -418,6 +419,54 @@ si_status si_spmm_f32(si_ctx* ctx, const si_operator* op, const float* x, float*
     si::Epilogue<float> ep;
     si::spmm_dev<float>(ex, o, x, y, static_cast<int>(k), static_cast<int>(k), ep, nullptr, true);
     SI_CUDA(cudaStreamSynchronize(ex.stream));
+  });
+}
+
+struct si_operator_plan {
+  int device = 0;
+  si::OpDev op;
+  si::RowBlocks rb;
+};
+
+si_status si_operator_plan_create(si_ctx* ctx, const si_operator* op, si_operator_plan** out) {
+  if (out != nullptr) *out = nullptr;
+  return guarded(ctx, [&] {
+    SI_REQUIRE(out != nullptr, SI_INVALID_ARGUMENT, "plan output pointer is null");
+    const si::Exec ex = ctx->ex();
+    std::unique_ptr<si_operator_plan> p(new si_operator_plan());
+    p->device = ctx->device;
+    p->op = op_of(op);
+    si::make_row_blocks(ex, p->op, p->rb);
+    p->rb.attach(p->op);
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
+    *out = p.release();
+  });
+}
+
+void si_operator_plan_destroy(si_operator_plan* plan) {
+  if (plan == nullptr) return;
+  cudaSetDevice(plan->device);
+  cudaDeviceSynchronize();
+  delete plan;
+}
+
+si_status si_spmm_planned(si_ctx* ctx, const si_operator_plan* plan, const double* x, double* y, uint32_t k) {
+  return guarded(ctx, [&] {
+    SI_REQUIRE(plan != nullptr, SI_INVALID_ARGUMENT, "plan is null");
+    SI_REQUIRE(plan->device == ctx->device, SI_INVALID_ARGUMENT, "plan was prepared on another device");
+    SI_REQUIRE(k >= 1, SI_INVALID_ARGUMENT, "k must be >= 1");
+    si::Epilogue<double> ep;
+    si::spmm_dev<double>(ctx->ex(), plan->op, x, y, static_cast<int>(k), static_cast<int>(k), ep);
+  });
+}
+
+si_status si_spmm_planned_f32(si_ctx* ctx, const si_operator_plan* plan, const float* x, float* y, uint32_t k) {
+  return guarded(ctx, [&] {
+    SI_REQUIRE(plan != nullptr, SI_INVALID_ARGUMENT, "plan is null");
+    SI_REQUIRE(plan->device == ctx->device, SI_INVALID_ARGUMENT, "plan was prepared on another device");
+    SI_REQUIRE(k >= 1, SI_INVALID_ARGUMENT, "k must be >= 1");
+    si::Epilogue<float> ep;
+    si::spmm_dev<float>(ctx->ex(), plan->op, x, y, static_cast<int>(k), static_cast<int>(k), ep, nullptr, true);
   });
 }
 
