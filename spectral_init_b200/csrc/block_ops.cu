@@ -6,6 +6,8 @@
 // All reductions are deterministic: every CTA writes its partial sums, and
 // the last CTA to finish (atomic ticket) adds them in CTA order.
 #include <algorithm>
+#include <string>
+#include <cstdlib>
 #include <vector>
 
 #include "si_internal.h"
@@ -242,6 +244,158 @@ __global__ void __launch_bounds__(G4_THREADS) k_gram4(const XT* __restrict__ X, 
     for (int w = 0; w < G4_WARPS; ++w) sum += red[w][e];
     partial[static_cast<int64_t>(blockIdx.x) * 288 + e] = sum;
   }
+}
+
+// Task-split Gram of a 4-column LOBPCG iteration.  Only the upper triangles
+// of S^T S and S^T AS are needed (156 of the 288 products a row of [S AS]
+// offers), so each of the CTA's four warps owns one share and computes it for
+// every row, one row per lane:
+//   warp 0: X^T [X R P]      (i in X, j >= i)    42 products from 12 values
+//   warp 1: [R P]^T [R P]    (i in R P, j >= i)  36 products from  8 values
+//   warp 2: X^T [AX AR AP]   (i in X, j >= i)    42 products from 16 values
+//   warp 3: [R P]^T [AR AP]  (i in R P, j >= i)  36 products from 16 values
+// A tile of 128 rows of the six blocks is loaded with coalesced 16-byte loads
+// (one warp reads 32 consecutive rows of one block), converted to f64 once
+// and stored with a row stride of 25 doubles, so a warp's 32 rows of one
+// column fall in distinct banks.  Accumulators stay in registers across all
+// tiles of the CTA; at the end each warp sums its lanes and the CTA writes
+// one 288-entry partial (the k_gram4 layout, unused entries zero) that
+// k_gram4_reduce adds in CTA order.
+constexpr int GT_TR = 128;
+constexpr int GT_STRIDE = 25;
+constexpr int GT_THREADS = 128;
+
+template <int TASK>
+struct GramTask;
+template <>
+struct GramTask<0> { static constexpr int I0 = 0, I1 = 4, TOFF = 0, N = 42; };
+template <>
+struct GramTask<1> { static constexpr int I0 = 4, I1 = 12, TOFF = 0, N = 36; };
+template <>
+struct GramTask<2> { static constexpr int I0 = 0, I1 = 4, TOFF = 12, N = 42; };
+template <>
+struct GramTask<3> { static constexpr int I0 = 4, I1 = 12, TOFF = 12, N = 36; };
+
+template <int TASK>
+__device__ __forceinline__ void gram_task_row(const double* __restrict__ row, double (&acc)[42]) {
+  using T = GramTask<TASK>;
+  double s[12], t[12];
+#pragma unroll
+  for (int i = T::I0; i < 12; ++i) s[i] = row[i];
+  if constexpr (T::TOFF != 0) {
+#pragma unroll
+    for (int j = T::I0; j < 12; ++j) t[j] = row[T::TOFF + j];
+  }
+  int e = 0;
+#pragma unroll
+  for (int i = T::I0; i < T::I1; ++i) {
+#pragma unroll
+    for (int j = i; j < 12; ++j) {
+      const double tj = (T::TOFF != 0) ? t[j] : s[j];
+      acc[e] = fma(s[i], tj, acc[e]);
+      ++e;
+    }
+  }
+}
+
+template <int TASK>
+__device__ __forceinline__ void gram_task_store(const double (&acc)[42], double* red) {
+  using T = GramTask<TASK>;
+  int e = 0;
+#pragma unroll
+  for (int i = T::I0; i < T::I1; ++i) {
+#pragma unroll
+    for (int j = i; j < 12; ++j) {
+      red[i * 24 + T::TOFF + j] = acc[e];
+      ++e;
+    }
+  }
+}
+
+template <class XT>
+__global__ void __launch_bounds__(GT_THREADS) k_gram4t(const XT* __restrict__ X, const XT* __restrict__ R,
+                                                        const XT* __restrict__ P, const XT* __restrict__ AX,
+                                                        const XT* __restrict__ AR, const XT* __restrict__ AP,
+                                                        int64_t n, double* __restrict__ partial,
+                                                        const int* __restrict__ stop) {
+  if (stop != nullptr && *stop != 0) return;
+  __shared__ double tile[GT_TR * GT_STRIDE];
+  __shared__ double red[288];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const XT* src[6] = {X, R, P, AX, AR, AP};
+  double acc[42];
+#pragma unroll
+  for (int e = 0; e < 42; ++e) acc[e] = 0.0;
+  for (int e = tid; e < 288; e += GT_THREADS) red[e] = 0.0;
+  constexpr int EPC = 16 / sizeof(XT);  // elements per 16-byte load
+  constexpr int CPR = 4 / EPC;          // loads per (row, block)
+  const int64_t ntiles = (n + GT_TR - 1) / GT_TR;
+  for (int64_t tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+    const int64_t row0 = tl * GT_TR;
+    // load: chunk c = (block b, half h, row r), rows fastest so a warp reads
+    // 32 consecutive rows of one block
+#pragma unroll 4
+    for (int c = tid; c < 6 * CPR * GT_TR; c += GT_THREADS) {
+      const int r = c % GT_TR;
+      const int bh = c / GT_TR;
+      const int b = bh / CPR, h = bh % CPR;
+      const int64_t row = row0 + r;
+      double v[EPC];
+      if (row < n) {
+        if constexpr (sizeof(XT) == 4) {
+          const float4 q = __ldcs(reinterpret_cast<const float4*>(src[b] + row * 4));
+          v[0] = q.x;
+          v[1] = q.y;
+          v[2] = q.z;
+          v[3] = q.w;
+        } else {
+          const double2 q = __ldcs(reinterpret_cast<const double2*>(src[b] + row * 4 + h * 2));
+          v[0] = q.x;
+          v[1] = q.y;
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < EPC; ++u) v[u] = 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < EPC; ++u) tile[r * GT_STRIDE + b * 4 + h * EPC + u] = v[u];
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int r = lane; r < GT_TR; r += 32) {
+      const double* row = tile + r * GT_STRIDE;
+      switch (warp) {
+        case 0: gram_task_row<0>(row, acc); break;
+        case 1: gram_task_row<1>(row, acc); break;
+        case 2: gram_task_row<2>(row, acc); break;
+        default: gram_task_row<3>(row, acc); break;
+      }
+    }
+    __syncthreads();
+  }
+  // sum each accumulator over the warp's lanes (fixed butterfly order)
+#pragma unroll
+  for (int e = 0; e < 42; ++e) {
+    double v = acc[e];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[e] = v;
+  }
+  if (lane == 0) {
+    switch (warp) {
+      case 0: gram_task_store<0>(acc, red); break;
+      case 1: gram_task_store<1>(acc, red); break;
+      case 2: gram_task_store<2>(acc, red); break;
+      default: gram_task_store<3>(acc, red); break;
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < 288; e += GT_THREADS) partial[static_cast<int64_t>(blockIdx.x) * 288 + e] = red[e];
+}
+
+bool gram4_old_forced() {
+  const char* e = std::getenv("SPECTRAL_INIT_GRAM");
+  return e != nullptr && std::string(e) == "tile";
 }
 
 // Adds the per-CTA partials of k_gram4 in CTA order (warp w takes CTAs w,
@@ -1209,8 +1363,29 @@ void gram_dev(const Exec& ex, GramWork& w, GramMode mode, const XT* const* blk, 
       gram_ld_launch<XT, 16>(ex, w, six, m, ns_out, n, out, stop);
     return;
   }
+  if ((iter || xonly) && m == 4 && ld == 4 && !gram4_old_forced()) {
+    // 4-column blocks: the task-split kernel
+    static std::atomic<int> resident_t[2][64];
+    const int ti = sizeof(XT) == 8 ? 1 : 0;
+    SI_REQUIRE(ex.device >= 0 && ex.device < 64, SI_INVALID_ARGUMENT, "gram: device ordinal");
+    if (resident_t[ti][ex.device] == 0) {
+      int r = 0;
+      SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gram4t<XT>, GT_THREADS, 0));
+      resident_t[ti][ex.device] = std::max(1, r);
+    }
+    const int64_t ntiles = (n + GT_TR - 1) / GT_TR;
+    const int grid = static_cast<int>(
+        std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(ex.sms) * resident_t[ti][ex.device].load())));
+    w.ensure(static_cast<size_t>(grid) * 288, ex.stream);
+    k_gram4t<XT><<<grid, GT_THREADS, 0, ex.stream>>>(six[0], six[1], six[2], six[3], six[4], six[5], n,
+                                                     w.partial.get(), stop);
+    SI_LAUNCH_CHECK();
+    k_gram4_reduce<<<9, 256, 0, ex.stream>>>(w.partial.get(), grid, ns_out, out, stop);
+    SI_LAUNCH_CHECK();
+    return;
+  }
   if ((iter || xonly) && m == 4 && ld == 4) {
-    // 4-column blocks
+    // 4-column blocks (SPECTRAL_INIT_GRAM=tile: the register-tiled kernel)
     // resident CTAs per SM from the stage memory (set once per device)
     static std::atomic<int> resident[2][64];
     const int ti = sizeof(XT) == 8 ? 1 : 0;

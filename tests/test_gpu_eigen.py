@@ -285,3 +285,24 @@ def test_lobpcg_wide_blocks(gpu_ctx, nc, block, precision):
     assert np.allclose(vecs.T @ vecs, np.eye(k), atol=1e-8)
     for j in range(k):
         assert resid(lap, vecs[:, j], vals[j]) < 1e-5
+
+
+@pytest.mark.parametrize("variant", ["task", "tile"])
+@pytest.mark.parametrize("small", ["warp", "cta"])
+def test_lobpcg_kernel_variants_agree(gpu_ctx, monkeypatch, variant, small):
+    """The 4-column LOBPCG iteration with either Gram kernel (task-split warps,
+    default; register-tiled, SPECTRAL_INIT_GRAM=tile) and either small step
+    (one warp in registers, default for up to 16 columns; one CTA,
+    SPECTRAL_INIT_SMALL_STEP=cta) converges to the dense eigenpairs."""
+    import spectral_init_b200 as si
+    if variant == "tile":
+        monkeypatch.setenv("SPECTRAL_INIT_GRAM", "tile")
+    if small == "cta":
+        monkeypatch.setenv("SPECTRAL_INIT_SMALL_STEP", "cta")
+    lap = load_csr("blobs_connected_2000", "comp_b_laplacian.npz")
+    cfg = si.SpectralInitConfig(force_level=1, tol=1e-10)
+    (vals, vecs), level = si.solve_eigenproblem_pub(lap, 2, 42, cfg, ctx=gpu_ctx)
+    w = np.linalg.eigvalsh(lap.toarray())[:3]
+    assert level == 1
+    assert np.all(np.abs(vals - w) < 1e-10), (vals, w)
+    assert O.max_eigenpair_residual(lap, vals, vecs) < 1e-9
