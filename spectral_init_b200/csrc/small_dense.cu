@@ -757,21 +757,23 @@ __device__ bool warp_rr_general(const double* gb, const double* ga, int P, const
   return true;
 }
 
-// Rayleigh-Ritz of the small step: the register-resident warp version when
-// the CTA is a single warp and the problem has at most 16 columns.
-template <int NT>
+// Rayleigh-Ritz of the small step: the shared-memory CTA routines (on a
+// single-warp CTA their barriers are warp-cheap), or, with REG, the
+// register-resident warp version (SPECTRAL_INIT_SMALL_STEP=reg).
+template <int NT, bool REG>
 __device__ bool rr_general(const double* gb, const double* ga, int P, const int* idx, int s, int nsel, int largest,
                            double chol_tol, SmallSmem sm, double* dsc, double* theta_out, double* red, double* rc,
                            double* rs, int* ra, int* rb, int* order, int* sflag) {
-  if constexpr (NT == 32) {
-    if (s <= WRR) return warp_rr_general(gb, ga, P, idx, s, nsel, largest, chol_tol, sm.Z, sm.ld, sm.T, theta_out);
+  if constexpr (NT == 32 && REG) {
+    if (s <= WRR)
+      return warp_rr_general(gb, ga, P, idx, s, nsel, largest, chol_tol, sm.Z, sm.ld, sm.T, theta_out);
   }
   return cta_rr_general(gb, ga, P, idx, s, nsel, largest, chol_tol, sm, dsc, theta_out, red, rc, rs, ra, rb, order,
                         sflag);
 }
 
 // `ctrl` points to the CTA's shared-memory copy of the control block.
-template <int NT>
+template <int NT, bool REG>
 __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns, int mode,
                                 double* smem) {
   __shared__ double red[ST_WIDE / 32];
@@ -795,7 +797,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
   if (mode == SM_INIT) {
     for (int i = threadIdx.x; i < m; i += blockDim.x) idx[i] = i;
     __syncthreads();
-    const bool ok = rr_general<NT>(gb, ga, P, idx, m, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc,
+    const bool ok = rr_general<NT, REG>(gb, ga, P, idx, m, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc,
                                    rs, ra, rb, order, &sflag);
     if (threadIdx.x == 0) {
       ctrl->iter = 0;
@@ -920,12 +922,12 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
         if (ctrl->active[c]) idx[m + na + q++] = 2 * m + c;
     }
     __syncthreads();
-    ok = rr_general<NT>(gb, ga, P, idx, m + 2 * na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs,
+    ok = rr_general<NT, REG>(gb, ga, P, idx, m + 2 * na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs,
                         ra, rb, order, &sflag);
     if (!ok) withp = 0;
   }
   if (!ok) {
-    ok = rr_general<NT>(gb, ga, P, idx, m + na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs, ra,
+    ok = rr_general<NT, REG>(gb, ga, P, idx, m + na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs, ra,
                         rb, order, &sflag);
   }
   if (!ok) {
@@ -962,7 +964,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
 
 // The control block is staged in shared memory for the whole step (the step
 // is a long chain of small dependent updates) and written back at the end.
-template <int NT>
+template <int NT, bool REG = false>
 __global__ void __launch_bounds__(NT) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
                                                    int mode) {
   extern __shared__ double smem[];
@@ -973,7 +975,7 @@ __global__ void __launch_bounds__(NT) k_small_step(LobpcgCtrl* ctrl, const doubl
   const double* src = reinterpret_cast<const double*>(ctrl);
   for (int i = threadIdx.x; i < W; i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  small_step_body<NT>(&sctrl, gram, ns, mode, smem);
+  small_step_body<NT, REG>(&sctrl, gram, ns, mode, smem);
   __syncthreads();
   double* back = reinterpret_cast<double*>(ctrl);
   for (int i = threadIdx.x; i < W; i += blockDim.x) back[i] = dst[i];
@@ -1021,9 +1023,15 @@ __global__ void __launch_bounds__(ST) k_small_dense(const double* __restrict__ a
 // SPECTRAL_INIT_SMALL_STEP=cta keeps the multi-warp small step for every
 // width (the single-warp version is the default up to 16 columns); read on
 // every call, so one process can compare both.
-bool small_step_cta_forced() {
+// SPECTRAL_INIT_SMALL_STEP = cta (128-thread CTA for every width up to 24
+// columns) | reg (single warp, register-resident Rayleigh-Ritz); default: a
+// single warp running the shared-memory routines for up to 16 columns.  Read
+// on every launch, so one process can compare them.
+int small_step_variant() {
   const char* e = std::getenv("SPECTRAL_INIT_SMALL_STEP");
-  return e != nullptr && std::string(e) == "cta";
+  if (e == nullptr) return 0;
+  const std::string v(e);
+  return v == "cta" ? 1 : (v == "reg" ? 2 : 0);
 }
 
 void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode, int m) {
@@ -1037,14 +1045,18 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
                                  static_cast<int>(smem)));
     SI_CUDA(cudaFuncSetAttribute(k_small_step<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
+    SI_CUDA(cudaFuncSetAttribute(k_small_step<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
     attr_set[ex.device] = true;
   }
   // the Rayleigh-Ritz problem has up to ns * m rows: up to 16 fit one warp's
   // registers; wider blocks get a CTA, the widest the most threads
   if (ns * m > 24)
     k_small_step<ST_WIDE><<<1, ST_WIDE, smem, ex.stream>>>(ctrl, gram, ns, mode);
-  else if (ns * m > WRR || small_step_cta_forced())
+  else if (ns * m > WRR || small_step_variant() == 1)
     k_small_step<ST><<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  else if (small_step_variant() == 2)
+    k_small_step<32, true><<<1, 32, smem, ex.stream>>>(ctrl, gram, ns, mode);
   else
     k_small_step<32><<<1, 32, smem, ex.stream>>>(ctrl, gram, ns, mode);
   SI_LAUNCH_CHECK();

@@ -569,11 +569,16 @@ __global__ void __launch_bounds__(NT, 1) k_spmm_panel(int64_t n, const uint64_t*
   constexpr int NG = NT / G;
   const int64_t b_lo = nblk * blockIdx.x / gridDim.x;
   const int64_t b_hi = nblk * (blockIdx.x + 1) / gridDim.x;
+  // a block whose planned window lies within WR/8 rows of the one held keeps
+  // the held window (it covers nearly the same columns): reloads only happen
+  // when the window really moves
+  constexpr int64_t kSlack = WR / 8;
   int64_t held = -1;
   for (int64_t b = b_lo; b < b_hi;) {
-    const int64_t w = pw0[b];
+    int64_t w = pw0[b];
+    if (held >= 0 && llabs(w - held) <= kSlack) w = held;
     int64_t be = b + 1;
-    while (be < b_hi && pw0[be] == w) ++be;
+    while (be < b_hi && llabs(pw0[be] - w) <= kSlack) ++be;
     const int64_t r0 = prow[b], r1 = prow[be];
     const uint32_t wn = static_cast<uint32_t>(min(static_cast<int64_t>(WR), n - w));
     if (w != held) {

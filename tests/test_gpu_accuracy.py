@@ -143,32 +143,76 @@ def test_config1_connected_default_tolerance_bound(gpu_ctx):
 def test_config1_pipeline_matches_oracle(gpu_ctx):
     """spectral_init on the 8-component graph with its points: the crate routes
     to embed_disconnected with the spectral meta-embedding (src/lib.rs:217-229,
-    src/multi_component.rs:16-312).  The meta-embedding gives several of these
-    components a range of (nearly) zero, so after the final scale to 10 their
-    points sit within the 1e-4 noise of one position: those are checked for
-    position and spread; components with a visible spread (> 1e-2) are
-    compared with the oracle's pre-noise embedding up to sign (each component
-    is solved densely, its eigenvalues are 0.01-0.03 apart)."""
+    src/multi_component.rs:16-312).  Here the cluster centroids are ~28 apart,
+    so every Gaussian affinity exp(-d^2) of the centroid graph underflows to 0:
+    the meta Laplacian is the identity, its eigenvectors are any orthonormal
+    basis, and the component positions (and with them the per-component
+    ranges) are not determined by the algorithm -- the crate's own output
+    depends on its eigensolver's choice.  What is determined is checked: the
+    output is finite and inside the box, and every component drawn with a
+    visible spread by both implementations has the same internal embedding up
+    to sign (each component is solved densely; its eigenvalues are 0.01-0.03
+    apart)."""
     import spectral_init_b200 as si
     x, g, _, _ = _config1(5.0)
+    labels, nc = O.find_components_fast(g)
+    cent = np.stack([x[labels == c].astype(np.float64).mean(0) for c in range(nc)])
+    d2 = ((cent[:, None, :] - cent[None, :, :]) ** 2).sum(2)
+    assert np.all(np.exp(-d2[~np.eye(nc, dtype=bool)]) == 0.0)  # the degenerate case described above
     out = si.spectral_init(g, 2, 42, data=x, ctx=gpu_ctx).astype(np.float64)
     pre = O.scale_coords(O.spectral_init_prenoise(g, 2, 42, data=x), 10.0).astype(np.float64)
-    labels, nc = O.find_components_fast(g)
-    spread_seen = 0
+    assert np.all(np.isfinite(out)) and float(np.max(np.abs(out))) <= 10.0 + 1e-3
+    compared = 0
     for c in range(nc):
         idx = np.nonzero(labels == c)[0]
-        assert np.allclose(np.abs(out[idx].mean(0)), np.abs(pre[idx].mean(0)), atol=5e-2), c
-        spread = float(pre[idx].std(0).min())
-        if spread < 1e-2:
-            assert float(out[idx].std(0).max()) < 1e-3 + 10 * spread, c
+        if min(float(out[idx].std(0).min()), float(pre[idx].std(0).min())) < 1e-2:
             continue
-        spread_seen += 1
+        compared += 1
         for ax in range(2):
             a = out[idx, ax] - out[idx, ax].mean()
             b = pre[idx, ax] - pre[idx, ax].mean()
             cos = abs(a @ b) / max(np.linalg.norm(a) * np.linalg.norm(b), 1e-300)
             assert cos > 0.99, (c, ax, cos)
-    assert spread_seen >= 1
+    assert compared >= 1
+
+
+def test_multi_component_positions_match_oracle(gpu_ctx):
+    """A multi-component graph whose centroid graph is connected (centroids
+    ~1.4 apart, affinities exp(-d^2) well above 0): the spectral meta-embedding
+    is determined, and the GPU pipeline's component positions and internal
+    embeddings match the oracle's pre-noise output up to per-axis sign."""
+    import scipy.sparse as sp
+    import spectral_init_b200 as si
+    rng = np.random.default_rng(5)
+    parts, pts = [], []
+    for c in range(9):
+        xc = G.gaussian_mixture(150, 1, 4, seed=100 + c, center_std=0.0) * 0.3
+        xc = xc + rng.normal(0.0, 0.5, size=(1, 4)).astype(np.float32)
+        parts.append(G.fuzzy_knn_graph(xc, 10))
+        pts.append(xc)
+    g = sp.block_diag(parts, format="csr").astype(np.float32)
+    g.sort_indices()
+    x = np.concatenate(pts).astype(np.float32)
+    labels, nc = O.find_components_fast(g)
+    assert nc == 9
+    out = si.spectral_init(g, 2, 42, data=x, ctx=gpu_ctx).astype(np.float64)
+    pre = O.scale_coords(O.spectral_init_prenoise(g, 2, 42, data=x), 10.0).astype(np.float64)
+    signs = []
+    for ax in range(2):
+        cs = np.array([out[labels == c, ax].mean() for c in range(nc)])
+        cp = np.array([pre[labels == c, ax].mean() for c in range(nc)])
+        sgn = 1.0 if np.abs(cs - cp).max() <= np.abs(cs + cp).max() else -1.0
+        signs.append(sgn)
+        assert np.abs(cs - sgn * cp).max() < 5e-3 * 10, (ax, cs, cp)
+    for c in range(nc):
+        idx = np.nonzero(labels == c)[0]
+        for ax in range(2):
+            a = out[idx, ax] - out[idx, ax].mean()
+            b = pre[idx, ax] - pre[idx, ax].mean()
+            if np.linalg.norm(b) < 1e-2 * np.sqrt(len(idx)):
+                continue
+            cos = abs(a @ b) / max(np.linalg.norm(a) * np.linalg.norm(b), 1e-300)
+            assert cos > 0.99, (c, ax, cos)
 
 
 # ---- the n = 200k configuration ------------------------------------------------------------
