@@ -536,66 +536,86 @@ __device__ __forceinline__ double sel16(const double (&a)[WRR], int i) {
   return v;
 }
 
-// One Jacobi round R (0..14) of the circle pairing of 16 columns.
-template <int R>
-__device__ __forceinline__ void warp_jacobi_round(double (&col)[WRR], int j, bool isv) {
-  constexpr int N1 = WRR - 1;
+// One Jacobi sweep over 16 columns as 15 rounds of one fixed shape: the pairs
+// are always the positions (2p, 2p + 1), and after every round the content
+// moves to new positions by the fixed permutation sigma of the circle method
+// (the player at position p goes to sigma[p]), so that every pair of columns
+// meets once per sweep and after 15 rounds every column is back where it
+// started.  With fixed pair positions every register index is a compile-time
+// constant while the round loop stays a runtime loop (one copy of the code).
+//   lane k < 16: column of C at position k (rows indexed by position);
+//   lane 16 + k: column of V at position k (rows in the original basis).
+// Moving to the next round permutes C's rows (a compile-time renaming of the
+// registers, C lanes only) and the columns of C and V (one shuffle per row).
+__device__ __constant__ int kJacSigmaInv[16] = {2, 1, 4, 0, 6, 3, 8, 5, 10, 7, 12, 9, 14, 11, 15, 13};
+
+__device__ __forceinline__ void warp_jacobi_sweep(double (&col)[WRR], int k, bool isv, int src_lane) {
   const unsigned full = 0xffffffffu;
-  const int q = (j == N1) ? R : (j == R ? N1 : (2 * R - j + 2 * N1) % N1);
-  const int a = min(j, q);
-  // rotation of the pair (a, b), formed by the A-lane of column a
-  const double djj = sel16(col, j);
-  const double dqq = __shfl_sync(full, djj, q);
-  const double ajq = sel16(col, q);
-  double c = 1.0, sn = 0.0;
-  if (!isv && j == a) {
-    const double app = djj, aqq = dqq, apq = ajq;
-    const double tiny = DBL_EPSILON * 1e-3;
-    if (fabs(apq) > 1e-300 && apq * apq > tiny * tiny * fabs(app * aqq)) {
-      const float d = static_cast<float>(aqq - app), h = static_cast<float>(2.0 * apq);
-      const float tf = (d >= 0.0f ? h : -h) / (fabsf(d) + sqrtf(fmaf(d, d, h * h)));
-      const float cf = rsqrtf(fmaf(tf, tf, 1.0f));
-      c = static_cast<double>(cf);
-      sn = static_cast<double>(tf) * static_cast<double>(cf);
+#pragma unroll 1
+  for (int round = 0; round < WRR - 1; ++round) {
+    // rotation of the pair (k & ~1, k | 1), formed by its even C lane
+    const double dkk = sel16(col, k);
+    const double dqq = __shfl_xor_sync(full, dkk, 1);
+    const double akq = sel16(col, k ^ 1);
+    double c = 1.0, sn = 0.0;
+    if (!isv && (k & 1) == 0) {
+      const double app = dkk, aqq = dqq, apq = akq;
+      const double tiny = DBL_EPSILON * 1e-3;
+      if (fabs(apq) > 1e-300 && apq * apq > tiny * tiny * fabs(app * aqq)) {
+        const float d = static_cast<float>(aqq - app), h = static_cast<float>(2.0 * apq);
+        const float tf = (d >= 0.0f ? h : -h) / (fabsf(d) + sqrtf(fmaf(d, d, h * h)));
+        const float cf = rsqrtf(fmaf(tf, tf, 1.0f));
+        c = static_cast<double>(cf);
+        sn = static_cast<double>(tf) * static_cast<double>(cf);
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const double f = fma(-0.5, fma(c, c, sn * sn), 1.5);
-        c *= f;
-        sn *= f;
+        for (int t = 0; t < 2; ++t) {
+          const double f = fma(-0.5, fma(c, c, sn * sn), 1.5);
+          c *= f;
+          sn *= f;
+        }
       }
     }
-  }
-  // column rotation of this lane's pair: new a = c a - s b ; new b = s a + c b
-  const double cp = __shfl_sync(full, c, a);
-  const double sp = __shfl_sync(full, sn, a);
-  const int partner = (isv ? WRR : 0) + q;
+    // column rotation: new even = c even - s odd ; new odd = s even + c odd
+    const double cp = __shfl_sync(full, c, k & ~1);
+    const double sp = __shfl_sync(full, sn, k & ~1);
+    const bool even = (k & 1) == 0;
 #pragma unroll
-  for (int i = 0; i < WRR; ++i) {
-    const double o = __shfl_sync(full, col[i], partner);
-    col[i] = (j == a) ? fma(cp, col[i], -sp * o) : fma(sp, o, cp * col[i]);
-  }
-  // row rotations of all 8 pairs (A lanes only; every lane joins the shuffles)
-#pragma unroll
-  for (int p = 0; p < WRR / 2; ++p) {
-    const int pa0 = (p == 0) ? R : (R + p) % N1;
-    const int pb0 = (p == 0) ? N1 : (R - p + N1) % N1;
-    const int pa = pa0 < pb0 ? pa0 : pb0;
-    const int pb = pa0 < pb0 ? pb0 : pa0;
-    const double cc = __shfl_sync(full, c, pa);
-    const double ss = __shfl_sync(full, sn, pa);
-    if (!isv) {
-      const double x = col[pa], y = col[pb];
-      col[pa] = fma(cc, x, -ss * y);
-      col[pb] = fma(ss, x, cc * y);
+    for (int i = 0; i < WRR; ++i) {
+      const double o = __shfl_xor_sync(full, col[i], 1);
+      col[i] = even ? fma(cp, col[i], -sp * o) : fma(sp, o, cp * col[i]);
     }
-  }
-}
-
-template <int R>
-__device__ __forceinline__ void warp_jacobi_rounds(double (&col)[WRR], int j, bool isv) {
-  if constexpr (R < WRR - 1) {
-    warp_jacobi_round<R>(col, j, isv);
-    warp_jacobi_rounds<R + 1>(col, j, isv);
+    // row rotations of the 8 pairs (C lanes)
+#pragma unroll
+    for (int p = 0; p < WRR / 2; ++p) {
+      const double cc = __shfl_sync(full, c, 2 * p);
+      const double ss = __shfl_sync(full, sn, 2 * p);
+      if (!isv) {
+        const double x = col[2 * p], y = col[2 * p + 1];
+        col[2 * p] = fma(cc, x, -ss * y);
+        col[2 * p + 1] = fma(ss, x, cc * y);
+      }
+    }
+    // next round's positions: rows of C renamed (row q takes row kJacSigmaInv[q]),
+    // columns of C and V moved
+    double t[WRR];
+    t[0] = isv ? col[0] : col[2];
+    t[1] = isv ? col[1] : col[1];
+    t[2] = isv ? col[2] : col[4];
+    t[3] = isv ? col[3] : col[0];
+    t[4] = isv ? col[4] : col[6];
+    t[5] = isv ? col[5] : col[3];
+    t[6] = isv ? col[6] : col[8];
+    t[7] = isv ? col[7] : col[5];
+    t[8] = isv ? col[8] : col[10];
+    t[9] = isv ? col[9] : col[7];
+    t[10] = isv ? col[10] : col[12];
+    t[11] = isv ? col[11] : col[9];
+    t[12] = isv ? col[12] : col[14];
+    t[13] = isv ? col[13] : col[11];
+    t[14] = isv ? col[14] : col[15];
+    t[15] = isv ? col[15] : col[13];
+#pragma unroll
+    for (int i = 0; i < WRR; ++i) col[i] = __shfl_sync(full, t[i], src_lane);
   }
 }
 
@@ -698,6 +718,7 @@ __device__ bool warp_rr_general(const double* gb, const double* ga, int P, const
     for (int i = 0; i < WRR; ++i) col[i] = (i == j) ? 1.0 : 0.0;  // V = I
   }
   __syncwarp();
+  const int src_lane = (isv ? WRR : 0) + kJacSigmaInv[j];
   for (int sweep = 0; sweep < 40; ++sweep) {
     double off = 0.0, dia = 0.0;
     if (!isv) {
@@ -713,7 +734,7 @@ __device__ bool warp_rr_general(const double* gb, const double* ga, int P, const
       dia += __shfl_xor_sync(full, dia, o);
     }
     if (!(off > jacobi_stop2(s) * dia)) break;
-    warp_jacobi_rounds<0>(col, j, isv);
+    warp_jacobi_sweep(col, j, isv, src_lane);
   }
   // eigenvalues (the diagonal) ranked among the live columns
   const double lam = isv ? 0.0 : sel16(col, j);
@@ -965,7 +986,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
 // The control block is staged in shared memory for the whole step (the step
 // is a long chain of small dependent updates) and written back at the end.
 template <int NT, bool REG = false>
-__global__ void __launch_bounds__(NT) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
+__global__ void __launch_bounds__(NT, 1) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
                                                    int mode) {
   extern __shared__ double smem[];
   __shared__ LobpcgCtrl sctrl;
