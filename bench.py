@@ -77,6 +77,9 @@ def parse_args():
                         "the n=1M graph with n_components=8 and the rSVD path; one JSON line each")
     p.add_argument("--dense", action="store_true",
                    help="the device dense eigensolver (level 0) at n = 300 / 1000 / 1900 instead, one JSON line")
+    p.add_argument("--learned-eval", type=int, default=0, metavar="G",
+                   help="one JSON line: learned vs random start (mixed precision, --tol) on G held-out graphs of the "
+                        "benchmark family (seeds --seed+1 .. --seed+G), iterations and device time")
     p.add_argument("--profile-solve", action="store_true",
                    help="one FP64 and one mixed eigensolve only (after one warm-up each), for ncu launch lists")
     return p.parse_args()
@@ -798,6 +801,67 @@ def run_configs(a):
     print(json.dumps(line), flush=True)
 
 
+def run_learned_eval(a):
+    """Learned vs random warm start on held-out graphs of the benchmark family
+    (n = --n, k = --k; the network was trained on n = 10k-200k graphs and never
+    saw these), mixed precision at --tol, device time with CUDA events."""
+    import argparse as _ap
+    import torch
+    import spectral_init_b200 as si
+    from spectral_init_b200._lib import SiConfig, SiReport
+    from spectral_init_b200.warm_start import WEIGHTS_PATH, DeviceLaplacian, WarmStartModel
+    dev = torch.device("cuda", 0)
+    ctx = si.Context(0)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(lib.si_ctx_stream(ctx.ptr), device=dev)
+    if not WEIGHTS_PATH.exists():
+        print(json.dumps({"learned_eval": True, "unavailable": "no trained weights"}))
+        return
+    model = WarmStartModel.load(ctx=ctx)
+    model.attach()
+    rows = []
+    for g_i in range(a.learned_eval):
+        ag = _ap.Namespace(**vars(a))
+        ag.seed = a.seed + 1 + g_i
+        ip, ix, dv = make_graph(ag, dev, 0)
+        lap = DeviceLaplacian((ip, ix, dv, a.n), ctx=ctx)
+        row = {"seed": ag.seed, "nnz": lap.nnz}
+        for name, warm in (("random", 0), ("learned", 1)):
+            cfg = SiConfig()
+            lib.si_config_default(C.byref(cfg))
+            cfg.precision = 1
+            cfg.warm_start = warm
+            cfg.tol = a.tol
+            k = a.nc + 1
+            vals = (C.c_double * k)()
+            vecs = torch.empty(a.n, k, dtype=torch.float64, device=dev)
+            lev = C.c_int32(-1)
+            rep = SiReport()
+            times = []
+            for _ in range(2):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.check(lib.si_solve_eigenproblem(ctx.ptr, C.byref(lap.op()), a.nc, a.seed, lap.sqrt_deg.data_ptr(),
+                                                    C.byref(cfg), vals, vecs.data_ptr(), C.byref(lev), C.byref(rep)))
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+            row[name] = {"ms": times[-1], "iterations": rep.iterations, "fp32_iterations": rep.fp32_iterations,
+                         "level": lev.value, "max_residual": rep.max_residual, "learned_start": rep.learned_start}
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+        del lap, ip, ix, dv
+    model.close()
+    it_l = statistics.mean(r["learned"]["iterations"] for r in rows)
+    it_r = statistics.mean(r["random"]["iterations"] for r in rows)
+    ms_l = statistics.mean(r["learned"]["ms"] for r in rows)
+    ms_r = statistics.mean(r["random"]["ms"] for r in rows)
+    print(json.dumps({"learned_eval": True, "workload": workload_name(a), "tol": a.tol, "graphs": len(rows),
+                      "mean_iterations_learned": it_l, "mean_iterations_random": it_r, "mean_ms_learned": ms_l,
+                      "mean_ms_random": ms_r, "rows": rows}))
+
+
 def run_dense(a):
     """One JSON line: the device dense eigensolver (level 0) on fuzzy-kNN graphs of a few sizes, device time
     per solve with CUDA events on the library's stream."""
@@ -845,6 +909,9 @@ def main():
         return
     if a.components and a.impl == "ours":
         run_components(a)
+        return
+    if a.learned_eval and a.impl == "ours":
+        run_learned_eval(a)
         return
     if a.dense and a.impl == "ours":
         run_dense(a)

@@ -125,60 +125,73 @@ def test_learned_solve_passes_the_fp64_gate(gpu_ctx):
     model.close()
 
 
-def test_trained_network_gain_on_held_out_graph(gpu_ctx, capsys):
-    """What the shipped (trained) network gains over the method without it, on a
-    graph of the training family that training never saw (n = 177 325, 28
-    anisotropic clusters with Dirichlet sizes in 96-D, k = 15, held-out seed):
-    its predicted block is closer to the FP64 eigenvectors than an untrained
-    network's (lower subspace loss), and the mixed-precision solve started from
-    it needs fewer LOBPCG iterations than the solve from the random start, at
-    the same FP64 residual gate.  (Across held-out graphs the iteration saving
-    varies and is not always positive; this graph is one data point.)"""
+def test_trained_network_gain_on_held_out_graphs(gpu_ctx, capsys):
+    """What the shipped (trained) network gains over the method without it, on
+    six graphs of the training family that training never saw (held-out seeds
+    900 000 + i; n 20k-120k, 5-100 anisotropic clusters with Dirichlet sizes,
+    10-100 dimensions, k in {10, 15, 30}; disconnected draws skipped):
+      * its predicted block is closer to the FP64 eigenvectors than an
+        untrained network's (lower subspace-projection loss) on average -- the
+        learned part learned something;
+      * every solve started from it passes the FP64 residual gate at level 1;
+      * the LOBPCG iterations learned vs random start are reported (mean and
+        per graph).  The iteration saving varies from graph to graph and is
+        not asserted."""
     import ctypes as C
     import torch
-    from spectral_init_b200 import synthetic
     from spectral_init_b200._lib import SiConfig, SiReport
+    from spectral_init_b200.train_warm_start import make_family_graph, n_components
     from spectral_init_b200.warm_start import WEIGHTS_PATH, DeviceLaplacian, WarmStartModel
     if not WEIGHTS_PATH.exists():
         pytest.skip("no trained weights in the package")
-    n = 177_325
-    x = synthetic.gaussian_mixture_gpu(n, 28, 96, 777_001, 2.0935246563775536, 0.018630844132704872,
-                                       anisotropic=True, dirichlet_alpha=0.5, device="cuda:0")
-    idx, dist = synthetic.knn_gpu(x, 15)
-    del x
-    sigma, rho = synthetic.smooth_knn_gpu(dist, 15)
-    g = synthetic.fuzzy_graph_gpu(idx, dist, sigma, rho)
-    lap = DeviceLaplacian((g[0], g[1], g[2], n), ctx=gpu_ctx)
     lib = gpu_ctx.lib
-
-    def solve(precision, warm):
-        cfg = SiConfig()
-        lib.si_config_default(C.byref(cfg))
-        cfg.precision = precision
-        cfg.warm_start = warm
-        vals = (C.c_double * 3)()
-        vecs = torch.empty(lap.n, 3, dtype=torch.float64, device="cuda:0")
-        level = C.c_int32(-1)
-        rep = SiReport()
-        torch.cuda.synchronize()
-        gpu_ctx.check(lib.si_solve_eigenproblem(gpu_ctx.ptr, C.byref(lap.op()), 2, 42, lap.sqrt_deg.data_ptr(),
-                                                C.byref(cfg), vals, vecs.data_ptr(), C.byref(level), C.byref(rep)))
-        return vecs, rep, level.value
-
-    v, _, level = solve(0, 0)
-    assert level == 1
     trained = WarmStartModel.load(ctx=gpu_ctx)
     untrained = WarmStartModel(0, ctx=gpu_ctx)
-    loss_trained = np.mean([trained.gradient(lap, v, seed=s)[0] for s in (1, 2, 3)])
-    loss_untrained = np.mean([untrained.gradient(lap, v, seed=s)[0] for s in (1, 2, 3)])
-    trained.attach()
-    _, rep_r, lev_r = solve(1, 0)
-    _, rep_l, lev_l = solve(1, 1)
-    with capsys.disabled():
-        print(f"\nheld-out n={n}: subspace loss trained {loss_trained:.3f} vs untrained {loss_untrained:.3f}; "
-              f"LOBPCG iterations learned {rep_l.iterations} vs random {rep_r.iterations}")
-    assert loss_trained < loss_untrained
-    assert lev_l == 1 and rep_l.max_residual < 1e-5 and rep_l.learned_start == 1
-    assert rep_l.iterations < rep_r.iterations
+    rng = np.random.default_rng(900_000)
+    rows = []
+    i = 0
+    while len(rows) < 6 and i < 20:
+        g, n, meta = make_family_graph(rng, 900_000 + i, "cuda:0", n_min=20_000, n_max=120_000)
+        i += 1
+        if n_components(gpu_ctx, g, n) != 1:
+            continue
+        lap = DeviceLaplacian((g[0], g[1], g[2], n), ctx=gpu_ctx)
+
+        def solve(precision, warm):
+            cfg = SiConfig()
+            lib.si_config_default(C.byref(cfg))
+            cfg.precision = precision
+            cfg.warm_start = warm
+            vals = (C.c_double * 3)()
+            vecs = torch.empty(lap.n, 3, dtype=torch.float64, device="cuda:0")
+            level = C.c_int32(-1)
+            rep = SiReport()
+            torch.cuda.synchronize()
+            gpu_ctx.check(lib.si_solve_eigenproblem(gpu_ctx.ptr, C.byref(lap.op()), 2, 42, lap.sqrt_deg.data_ptr(),
+                                                    C.byref(cfg), vals, vecs.data_ptr(), C.byref(level),
+                                                    C.byref(rep)))
+            return vecs, rep, level.value
+
+        v, _, level = solve(0, 0)
+        if level != 1:
+            continue
+        lt = float(np.mean([trained.gradient(lap, v, seed=s)[0] for s in (1, 2)]))
+        lu = float(np.mean([untrained.gradient(lap, v, seed=s)[0] for s in (1, 2)]))
+        trained.attach()
+        _, rep_r, _ = solve(1, 0)
+        _, rep_l, lev_l = solve(1, 1)
+        trained.detach()
+        assert lev_l == 1 and rep_l.max_residual < 1e-5
+        rows.append((n, lt, lu, rep_l.iterations, rep_r.iterations, rep_l.learned_start))
     trained.close()
     untrained.close()
+    assert len(rows) >= 5
+    lt = np.mean([r[1] for r in rows])
+    lu = np.mean([r[2] for r in rows])
+    it_l = np.mean([r[3] for r in rows])
+    it_r = np.mean([r[4] for r in rows])
+    with capsys.disabled():
+        print(f"\nheld-out family graphs: mean subspace loss trained {lt:.3f} vs untrained {lu:.3f}; "
+              f"mean LOBPCG iterations learned {it_l:.1f} vs random {it_r:.1f}; per graph (n, learned, random): "
+              + ", ".join(f"({r[0]}, {r[3]}, {r[4]})" for r in rows))
+    assert lt < lu
