@@ -449,7 +449,10 @@ __global__ void __launch_bounds__(kPlanThreads) k_panel_windows(int64_t n, const
       const int64_t st = static_cast<int64_t>(0xffffffffu - static_cast<unsigned>(k & 0xffffffffLL));
       int64_t start = st * bin;
       start = min(start, max(n - static_cast<int64_t>(W), int64_t(0)));
-      w0[b] = max(start, int64_t(0));
+      // a block whose best window holds less than half of its entries gains
+      // little from one: marked -1, it is computed with global gathers only
+      const long long inside = k >> 32;
+      w0[b] = (2 * inside < static_cast<long long>(p1 - p0)) ? int64_t(-1) : max(start, int64_t(0));
     }
     __syncthreads();
   }
@@ -576,9 +579,13 @@ __global__ void __launch_bounds__(NT, 1) k_spmm_panel(int64_t n, const uint64_t*
   int64_t held = -1;
   for (int64_t b = b_lo; b < b_hi;) {
     int64_t w = pw0[b];
+    if (w < 0) {  // no useful window: left to the second phase
+      ++b;
+      continue;
+    }
     if (held >= 0 && llabs(w - held) <= kSlack) w = held;
     int64_t be = b + 1;
-    while (be < b_hi && llabs(pw0[be] - w) <= kSlack) ++be;
+    while (be < b_hi && pw0[be] >= 0 && llabs(pw0[be] - w) <= kSlack) ++be;
     const int64_t r0 = prow[b], r1 = prow[be];
     const uint32_t wn = static_cast<uint32_t>(min(static_cast<int64_t>(WR), n - w));
     if (w != held) {
@@ -595,6 +602,15 @@ __global__ void __launch_bounds__(NT, 1) k_spmm_panel(int64_t n, const uint64_t*
       spmm_row_panel<VT, XT, LD, G>(row, indptr[row], indptr[row + 1], indices, vals, diag, x, panel,
                                     static_cast<uint32_t>(w), wn, y, ep, sub, mask, writer);
     b = be;
+  }
+  // second phase: blocks without a window (rows whose columns scatter over
+  // the whole graph), spread over all CTAs, global gathers only
+  for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
+    if (pw0[b] >= 0) continue;
+    const int64_t r0 = prow[b], r1 = prow[b + 1];
+    for (int64_t row = r0 + group; row < r1; row += NG)
+      spmm_row_panel<VT, XT, LD, G>(row, indptr[row], indptr[row + 1], indices, vals, diag, x, panel, 0u, 0u, y,
+                                    ep, sub, mask, writer);
   }
 }
 
