@@ -56,6 +56,10 @@ def parse_args():
                    help="LOBPCG tolerance of the mixed / learned legs (the headline): tight enough that their "
                         "subspace is within 1e-4 of the FP64 oracle on this graph; the plain FP64 leg runs at "
                         "the crate's 1e-5 (the drop-in)")
+    p.add_argument("--switch-tol", type=float, default=0.0,
+                   help="mixed precision: residual at which the f32 phase hands over to f64 (0: the library default)")
+    p.add_argument("--learned-filter", type=int, default=0,
+                   help="1: apply the Chebyshev start filter to the learned block as well")
     p.add_argument("--no-oracle", action="store_true", help="skip the CPU ARPACK accuracy oracle")
     p.add_argument("--accuracy-sweep", action="store_true",
                    help="one JSON line: mixed/learned/FP64 solves at several tolerances, time and error vs the oracle")
@@ -317,12 +321,15 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         legs.append(("fp64_same_tol", 0, 0, a.tol))
     head = "learned" if model is not None else "mixed"
 
-    def solve(precision: int, warm: int = 0, tol: float = 0.0):
+    def solve(precision: int, warm: int = 0, tol: float = 0.0, switch_tol: float | None = None,
+              learned_filter: int | None = None):
         cfg = SiConfig()
         lib.si_config_default(C.byref(cfg))
         cfg.precision = precision
         cfg.warm_start = warm
         cfg.tol = tol
+        cfg.mixed_switch_tol = a.switch_tol if switch_tol is None else switch_tol
+        cfg.learned_filter = a.learned_filter if learned_filter is None else learned_filter
         vals = (C.c_double * k)()
         vecs = torch.empty(n, k, dtype=torch.float64, device=dev)
         level = C.c_int32(-1)
@@ -366,6 +373,21 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
                     r["vs_oracle"] = oracle_errors(oracle, vals, vecs)
                 rows.append(r)
                 print(json.dumps(r), flush=True)
+        # at the headline tolerance: where the f32 phase hands over, and the start filter on the learned block
+        for name, prec, warm in (("mixed", 1, 0), ("learned", 1, 1)):
+            if warm and model is None:
+                continue
+            for sw in (1e-4, 1e-5, 3e-6):
+                for lf in ((0, 1) if warm else (0,)):
+                    solve(prec, warm, a.tol, sw, lf)
+                    ms, vals, vecs, level, rep = solve(prec, warm, a.tol, sw, lf)
+                    r = {"leg": name, "tol": a.tol, "switch_tol": sw, "learned_filter": lf, "ms": ms,
+                         "iterations": rep.iterations, "fp32_iterations": rep.fp32_iterations,
+                         "max_residual": rep.max_residual, "learned_start": rep.learned_start}
+                    if oracle is not None:
+                        r["vs_oracle"] = oracle_errors(oracle, vals, vecs)
+                    rows.append(r)
+                    print(json.dumps(r), flush=True)
         print(json.dumps({"accuracy_sweep": True, "n": n, "nnz": nnz, "rows": rows,
                           "oracle": None if oracle is None else oracle["summary"]}))
         return
