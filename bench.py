@@ -856,6 +856,7 @@ def run_learned_eval(a):
             cfg.precision = 1
             cfg.warm_start = warm
             cfg.tol = a.tol
+            cfg.learned_filter = a.learned_filter
             k = a.nc + 1
             vals = (C.c_double * k)()
             vecs = torch.empty(a.n, k, dtype=torch.float64, device=dev)
@@ -882,6 +883,7 @@ def run_learned_eval(a):
     ms_l = statistics.mean(r["learned"]["ms"] for r in rows)
     ms_r = statistics.mean(r["random"]["ms"] for r in rows)
     print(json.dumps({"learned_eval": True, "workload": workload_name(a), "tol": a.tol, "graphs": len(rows),
+                      "learned_filter": a.learned_filter,
                       "mean_iterations_learned": it_l, "mean_iterations_random": it_r, "mean_ms_learned": ms_l,
                       "mean_ms_random": ms_r, "rows": rows}))
 
