@@ -481,7 +481,11 @@ __device__ __forceinline__ void smem_row(const XT* p, double (&v)[LD]) {
 }
 
 // One row by a group of G lanes, gathers from the window [w, w + wn) when the
-// column falls inside it (spmm_row otherwise).
+// column falls inside it (global memory otherwise).  The row's streams are
+// addressed from its start with 32-bit offsets (the kernel is used only for
+// operators with fewer than 2^31 entries), so the per-entry work is two
+// streaming loads, one 16/32-byte gather and the LD fused multiply-adds; the
+// own-row epilogue loads are issued before the gathers.
 template <class VT, class XT, int LD, int G>
 __device__ __forceinline__ void spmm_row_panel(int64_t row, uint64_t s, uint64_t e, const uint32_t* __restrict__ idx,
                                                const VT* __restrict__ val, double diag, const XT* __restrict__ x,
@@ -503,26 +507,29 @@ __device__ __forceinline__ void spmm_row_panel(int64_t row, uint64_t s, uint64_t
       if (ep.z3) addz[c] = fma(ep.delta, static_cast<double>(ep.z3[off]), addz[c]);
     }
   }
+  const uint32_t* __restrict__ ip = idx + s;
+  const VT* __restrict__ vp = val + s;
+  const int len = static_cast<int>(e - s);
   double acc[LD];
 #pragma unroll
   for (int c = 0; c < LD; ++c) acc[c] = 0.0;
-  for (uint64_t b0 = s + sub; b0 < e; b0 += static_cast<uint64_t>(G) * U) {
+  for (int t0 = sub; t0 < len; t0 += G * U) {
     uint32_t jj[U];
     double vv[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const uint64_t k = b0 + static_cast<uint64_t>(u) * G;
-      const bool ok = k < e;
-      jj[u] = ok ? ld_stream(idx + k) : 0u;
-      vv[u] = ok ? static_cast<double>(ld_stream(val + k)) : 0.0;
+      const int t = t0 + u * G;
+      const bool ok = t < len;
+      jj[u] = ok ? ld_stream(ip + t) : 0u;
+      vv[u] = ok ? static_cast<double>(ld_stream(vp + t)) : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      if (b0 + static_cast<uint64_t>(u) * G < e) {
+      if (t0 + u * G < len) {
         double xr[LD];
         const uint32_t d = jj[u] - w;
         if (d < wn) smem_row<XT, LD>(panel + static_cast<size_t>(d) * LD, xr);
-        else RowLoad<XT, LD>::run(x + static_cast<int64_t>(jj[u]) * LD, xr);
+        else RowLoad<XT, LD>::run(x + static_cast<size_t>(jj[u]) * LD, xr);
 #pragma unroll
         for (int c = 0; c < LD; ++c) acc[c] = fma(vv[u], xr[c], acc[c]);
       }
@@ -943,6 +950,7 @@ bool launch_panel(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, 
   constexpr int WR = panel_rows<XT, LD>();
   constexpr int NT = panel_threads<XT, LD>();
   constexpr int G = 4;
+  if (op.nnz >= (int64_t(1) << 31)) return false;  // 32-bit offsets within a row
   const int64_t* w0 = panel_windows(ex, op, WR);
   if (w0 == nullptr) return false;
   const int smem = WR * LD * static_cast<int>(sizeof(XT));
