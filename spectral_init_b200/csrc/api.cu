@@ -437,6 +437,7 @@ si_status si_operator_plan_create(si_ctx* ctx, const si_operator* op, si_operato
     p->device = ctx->device;
     p->op = op_of(op);
     si::make_row_blocks(ex, p->op, p->rb);
+    p->rb.sell_ok = true;
     p->rb.attach(p->op);
     SI_CUDA(cudaStreamSynchronize(ex.stream));
     *out = p.release();

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -66,6 +67,22 @@ struct PanelWindows {
   DevBuf<int64_t> w0;
 };
 
+// Sliced-ELL copy of an operator for the sliced SpMM.  Rows are sorted by
+// length (longest first) inside windows of kSellSortRows consecutive rows and
+// cut into slices of 32; slot (s, j, r), at slice_ptr[s] + 32 j + r, holds
+// entry j of row perm[32 s + r] (plen[32 s + r] entries; slots past a row's
+// length hold index 0 and value 0, rows past n have perm = 0xffffffff).
+// Slice s is as wide as its longest row.
+constexpr int kSellSortRows = 256;
+struct SellLayout {
+  int64_t n_slices = 0;
+  uint64_t slots = 0;
+  DevBuf<uint64_t> slice_ptr;  // n_slices + 1
+  DevBuf<uint32_t> perm, plen, idx;
+  DevBuf<float> v32;
+  DevBuf<double> v64;
+};
+
 // Row partition of an operator for the tiled SpMM (device array of
 // n_blocks + 1 row starts, owned by the caller).
 struct RowBlocks {
@@ -75,6 +92,11 @@ struct RowBlocks {
   // windows of the panel SpMM, one entry per window size used (built lazily
   // by the first SpMM that needs them outside stream capture)
   mutable std::vector<PanelWindows> windows;
+  // sliced-ELL copy (built lazily outside stream capture, only when sell_ok:
+  // owners that apply the operator many times with unchanged values)
+  bool sell_ok = false;
+  mutable std::unique_ptr<SellLayout> sell;
+  mutable bool sell_failed = false;
   void attach(OpDev& op) const {
     op.row_blocks = starts.get();
     op.block_ptr = ptrs.get();

@@ -323,6 +323,7 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
   OpDev op = op_in;
   if (op.row_blocks == nullptr && op.n > 0) {
     make_row_blocks(ex, op, row_blocks_);
+    row_blocks_.sell_ok = true;
     row_blocks_.attach(op);
   }
   const int64_t n = op.n;
@@ -475,6 +476,7 @@ bool sinv_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64
   OpDev op = op_in;
   if (op.row_blocks == nullptr && op.n > 0) {
     make_row_blocks(ex, op, row_blocks_);
+    row_blocks_.sell_ok = true;
     row_blocks_.attach(op);
   }
   const int64_t n = op.n;
@@ -608,6 +610,7 @@ void rsvd_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint64
   OpDev op = op_in;
   if (op.row_blocks == nullptr && op.n > 0) {
     make_row_blocks(ex, op, row_blocks_);
+    row_blocks_.sell_ok = true;
     row_blocks_.attach(op);
   }
   const int64_t n = op.n;
@@ -685,6 +688,7 @@ void solve_eigenproblem_dev(const Exec& ex, const OpDev& op_in, int n_components
   OpDev op = op_in;
   if (op.row_blocks == nullptr && op.n > 0) {
     make_row_blocks(ex, op, row_blocks_);
+    row_blocks_.sell_ok = true;
     row_blocks_.attach(op);
   }
   const int64_t n = op.n;

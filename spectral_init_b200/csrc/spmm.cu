@@ -968,6 +968,267 @@ bool launch_panel(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, 
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Sliced SpMM.  One lane owns one row of a 32-row slice of the sliced-ELL copy
+// (SellLayout), so a warp's index and value loads are two coalesced 128-byte
+// requests per 32 entries, no lane waits on another's row bounds, and the row
+// sum needs no cross-lane reduction: per stored entry the warp issues about
+// half an instruction besides the gather and the FMAs (the CSR kernels issue
+// three).  Rows are sorted by length inside 256-row windows so a slice is
+// about as wide as its average row.  Persistent CTAs (one or two per SM) own
+// contiguous slice ranges balanced by slot count; with L1-cached gathers the
+// x rows a CTA's neighbourhood touches stay in the SM's L1 for graphs whose
+// node order keeps neighbours near (kNN graphs of clustered data, locality
+// orders).
+
+// Rank sort of each window of kSellSortRows rows by length (longest first,
+// ties by row): one CTA a window.
+__global__ void __launch_bounds__(kSellSortRows) k_sell_sort(int64_t n, int64_t n_pad,
+                                                              const uint64_t* __restrict__ indptr,
+                                                              uint32_t* __restrict__ perm,
+                                                              uint32_t* __restrict__ plen) {
+  __shared__ long long len_s[kSellSortRows];
+  const int i = threadIdx.x;
+  const int64_t row = static_cast<int64_t>(blockIdx.x) * kSellSortRows + i;
+  const long long len = row < n ? static_cast<long long>(indptr[row + 1] - indptr[row]) : -1;
+  len_s[i] = len;
+  __syncthreads();
+  int rank = 0;
+  for (int j = 0; j < kSellSortRows; ++j) {
+    const long long o = len_s[j];
+    rank += (o > len || (o == len && j < i)) ? 1 : 0;
+  }
+  const int64_t pos = static_cast<int64_t>(blockIdx.x) * kSellSortRows + rank;
+  if (pos < n_pad) {
+    perm[pos] = row < n ? static_cast<uint32_t>(row) : 0xffffffffu;
+    plen[pos] = row < n ? static_cast<uint32_t>(len) : 0u;
+  }
+}
+
+// Slots of each slice (32 x its first, longest row), one more zero entry for
+// the scan.
+__global__ void k_sell_widths(int64_t n_slices, const uint32_t* __restrict__ plen, uint64_t* __restrict__ cnt) {
+  for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s <= n_slices;
+       s += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    cnt[s] = s < n_slices ? 32ull * plen[s * 32] : 0ull;
+}
+
+// Copy of the index and value streams into slots: one warp a slice.
+__global__ void k_sell_fill(int64_t n_slices, const uint64_t* __restrict__ slice_ptr,
+                            const uint32_t* __restrict__ perm, const uint32_t* __restrict__ plen,
+                            const uint64_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
+                            const float* __restrict__ v32, const double* __restrict__ v64,
+                            uint32_t* __restrict__ sidx, float* __restrict__ s32, double* __restrict__ s64) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x / 32);
+  for (int64_t s = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / 32; s < n_slices; s += warps) {
+    const uint64_t base = slice_ptr[s];
+    const uint64_t w = (slice_ptr[s + 1] - base) / 32;
+    const uint32_t row = perm[s * 32 + lane];
+    const uint64_t len = plen[s * 32 + lane];
+    const uint64_t src = row != 0xffffffffu ? indptr[row] : 0;
+    for (uint64_t j = 0; j < w; ++j) {
+      const uint64_t slot = base + 32 * j + lane;
+      const bool ok = j < len;
+      sidx[slot] = ok ? indices[src + j] : 0u;
+      if (s32 != nullptr) s32[slot] = ok ? v32[src + j] : 0.0f;
+      if (s64 != nullptr) s64[slot] = ok ? v64[src + j] : 0.0;
+    }
+  }
+}
+
+// x row gather for the sliced kernel: L1-cached (.nc) or L2-only (.cg).
+template <class XT, int LD, bool L1>
+struct SellRowLoad;
+template <int LD, bool L1>
+struct SellRowLoad<double, LD, L1> {
+  __device__ __forceinline__ static void run(const double* p, double (&v)[LD]) {
+#pragma unroll
+    for (int q = 0; q < LD / 4; ++q) {
+      double a, b, c, d;
+      if constexpr (L1)
+        asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p + 4 * q));
+      else
+        asm volatile("ld.global.cg.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p + 4 * q));
+      v[4 * q + 0] = a;
+      v[4 * q + 1] = b;
+      v[4 * q + 2] = c;
+      v[4 * q + 3] = d;
+    }
+  }
+};
+template <int LD, bool L1>
+struct SellRowLoad<float, LD, L1> {
+  __device__ __forceinline__ static void run(const float* p, double (&v)[LD]) {
+#pragma unroll
+    for (int q = 0; q < LD / 4; ++q) {
+      const float4* a = reinterpret_cast<const float4*>(p + 4 * q);
+      const float4 t = L1 ? __ldg(a) : __ldcg(a);
+      v[4 * q + 0] = t.x;
+      v[4 * q + 1] = t.y;
+      v[4 * q + 2] = t.z;
+      v[4 * q + 3] = t.w;
+    }
+  }
+};
+
+// First slice whose slot offset is >= target (n_slices when none).
+__device__ __forceinline__ int64_t sell_bound(const uint64_t* __restrict__ slice_ptr, int64_t n_slices,
+                                              uint64_t target) {
+  int64_t lo = 0, hi = n_slices;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) / 2;
+    if (slice_ptr[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <class VT, class XT, int LD, int U, int NT, bool L1>
+__global__ void __launch_bounds__(NT, 1) k_spmm_sell(int64_t n_slices, const uint64_t* __restrict__ slice_ptr,
+                                                     const uint32_t* __restrict__ perm,
+                                                     const uint32_t* __restrict__ plen,
+                                                     const uint32_t* __restrict__ sidx, const VT* __restrict__ sval,
+                                                     double diag, const XT* __restrict__ x, XT* __restrict__ y,
+                                                     Epilogue<XT> ep, const int* __restrict__ stop) {
+  if (stop != nullptr && *stop != 0) return;
+  constexpr int NW = NT / 32;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x / 32;
+  const uint64_t total = slice_ptr[n_slices];
+  const int64_t s_lo = blockIdx.x == 0 ? 0 : sell_bound(slice_ptr, n_slices, total * blockIdx.x / gridDim.x);
+  const int64_t s_hi = blockIdx.x + 1 == gridDim.x ? n_slices
+                                                    : sell_bound(slice_ptr, n_slices, total * (blockIdx.x + 1) / gridDim.x);
+  for (int64_t s = s_lo + warp; s < s_hi; s += NW) {
+    const uint64_t base = slice_ptr[s];
+    const int64_t w = static_cast<int64_t>((slice_ptr[s + 1] - base) / 32);
+    const uint32_t row = perm[s * 32 + lane];
+    const int64_t len = plen[s * 32 + lane];
+    const uint32_t* __restrict__ ip = sidx + base + lane;
+    const VT* __restrict__ vp = sval + base + lane;
+    double acc[LD];
+#pragma unroll
+    for (int c = 0; c < LD; ++c) acc[c] = 0.0;
+    for (int64_t j0 = 0; j0 < w; j0 += U, ip += 32 * U, vp += 32 * U) {
+      uint32_t jj[U];
+      double vv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool ok = j0 + u < w;
+        jj[u] = ok ? ld_stream(ip + 32 * u) : 0u;
+        vv[u] = ok ? static_cast<double>(ld_stream(vp + 32 * u)) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (j0 + u < len) {
+          double xr[LD];
+          SellRowLoad<XT, LD, L1>::run(x + static_cast<size_t>(jj[u]) * LD, xr);
+#pragma unroll
+          for (int c = 0; c < LD; ++c) acc[c] = fma(vv[u], xr[c], acc[c]);
+        }
+      }
+    }
+    if (row != 0xffffffffu) {
+      const size_t off = static_cast<size_t>(row) * LD;
+#pragma unroll
+      for (int c = 0; c < LD; ++c) {
+        const double own = diag * static_cast<double>(x[off + c]);
+        double addz = 0.0;
+        if (ep.z1) addz = ep.beta * static_cast<double>(ep.z1[off + c]);
+        if (ep.z2) addz = fma(ep.gamma, static_cast<double>(ep.z2[off + c]), addz);
+        if (ep.z3) addz = fma(ep.delta, static_cast<double>(ep.z3[off + c]), addz);
+        y[off + c] = static_cast<XT>(fma(ep.alpha, own + acc[c], addz));
+      }
+    }
+  }
+}
+
+// The sliced-ELL copy of the operator (built on first use, outside stream
+// capture, for owners that allow it; null when not available).
+const SellLayout* sell_layout(const Exec& ex, const OpDev& op) {
+  if (op.panels == nullptr || !op.panels->sell_ok || op.panels->sell_failed) return nullptr;
+  if (op.panels->sell) return op.panels->sell.get();
+  if (op.n <= 0 || op.n >= int64_t(0xffffffff) || op.nnz >= (int64_t(1) << 32)) return nullptr;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  SI_CUDA(cudaStreamIsCapturing(ex.stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return nullptr;
+  auto L = std::make_unique<SellLayout>();
+  L->n_slices = (op.n + 31) / 32;
+  const int64_t n_pad = L->n_slices * 32;
+  const int64_t n_win = (op.n + kSellSortRows - 1) / kSellSortRows;
+  L->perm.alloc(static_cast<size_t>(n_pad), ex.stream);
+  L->plen.alloc(static_cast<size_t>(n_pad), ex.stream);
+  k_sell_sort<<<static_cast<unsigned>(n_win), kSellSortRows, 0, ex.stream>>>(op.n, n_pad, op.indptr, L->perm.get(),
+                                                                              L->plen.get());
+  SI_LAUNCH_CHECK();
+  DevBuf<uint64_t> cnt(static_cast<size_t>(L->n_slices + 1), ex.stream);
+  const int g1 = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((L->n_slices + 256) / 256, int64_t(ex.sms) * 8)));
+  k_sell_widths<<<g1, 256, 0, ex.stream>>>(L->n_slices, L->plen.get(), cnt.get());
+  SI_LAUNCH_CHECK();
+  L->slice_ptr.alloc(static_cast<size_t>(L->n_slices + 1), ex.stream);
+  L->slots = exclusive_scan_u64(ex, cnt.get(), L->slice_ptr.get(), L->n_slices);
+  // the copy must fit beside the solver's work buffers: at most a quarter of
+  // the free memory, and no more than twice the stored entries
+  const size_t per_slot = 4 + (op.v32 ? 4 : 0) + (op.v64 ? 8 : 0);
+  size_t free_b = 0, total_b = 0;
+  SI_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  if (L->slots > 2 * static_cast<uint64_t>(std::max<int64_t>(op.nnz, 1)) + 32ull * L->n_slices ||
+      L->slots * per_slot > free_b / 4) {
+    op.panels->sell_failed = true;
+    return nullptr;
+  }
+  L->idx.alloc(static_cast<size_t>(L->slots), ex.stream);
+  if (op.v32) L->v32.alloc(static_cast<size_t>(L->slots), ex.stream);
+  if (op.v64) L->v64.alloc(static_cast<size_t>(L->slots), ex.stream);
+  const int g2 = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((L->n_slices + 7) / 8, int64_t(ex.sms) * 16)));
+  k_sell_fill<<<g2, 256, 0, ex.stream>>>(L->n_slices, L->slice_ptr.get(), L->perm.get(), L->plen.get(), op.indptr,
+                                          op.indices, op.v32, op.v64, L->idx.get(), L->v32.get(), L->v64.get());
+  SI_LAUNCH_CHECK();
+  op.panels->sell = std::move(L);
+  return op.panels->sell.get();
+}
+
+template <class XT, int LD>
+constexpr int sell_threads() {
+  return (LD * sizeof(XT) <= 16) ? 1024 : 512;
+}
+template <class XT, int LD>
+constexpr int sell_unroll() {
+  return (LD * sizeof(XT) <= 32) ? 4 : (LD * sizeof(XT) <= 64 ? 2 : 1);
+}
+
+template <class VT, class XT, int LD, bool L1>
+bool launch_sell(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
+                 const int* stop) {
+  const SellLayout* L = sell_layout(ex, op);
+  if (L == nullptr) return false;
+  const VT* sval;
+  if constexpr (std::is_same<VT, float>::value) {
+    if (vals != op.v32) return false;
+    sval = L->v32.get();
+  } else {
+    if (vals != op.v64) return false;
+    sval = L->v64.get();
+  }
+  if (sval == nullptr) return false;
+  constexpr int NT = sell_threads<XT, LD>();
+  constexpr int U = sell_unroll<XT, LD>();
+  static std::atomic<int> ready[128];
+  const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
+  if (ready[dev] == 0) {
+    SI_CUDA(cudaFuncSetAttribute(k_spmm_sell<VT, XT, LD, U, NT, L1>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, 0));
+    ready[dev] = 1;
+  }
+  const int per_sm = 2048 / NT;
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(L->n_slices, int64_t(ex.sms) * per_sm)));
+  k_spmm_sell<VT, XT, LD, U, NT, L1><<<grid, NT, 0, ex.stream>>>(L->n_slices, L->slice_ptr.get(), L->perm.get(),
+                                                                 L->plen.get(), L->idx.get(), sval, op.diag, x, y, ep,
+                                                                 stop);
+  SI_LAUNCH_CHECK();
+  return true;
+}
+
 // choice < 100: direct kernel with `choice` lanes per row; 100 + g: tiled kernel
 template <class VT, class XT, int LD>
 void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
@@ -975,6 +1236,12 @@ void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const 
   if (g == 300) {
     if (launch_panel<VT, XT, LD>(ex, op, vals, x, y, ep, stop)) return;
     g = spmm_group_lanes(op);  // no windows (inside a capture before first use): direct kernel
+  }
+  if (g == 400 || g == 401) {
+    if (g == 400 ? launch_sell<VT, XT, LD, false>(ex, op, vals, x, y, ep, stop)
+                 : launch_sell<VT, XT, LD, true>(ex, op, vals, x, y, ep, stop))
+      return;
+    g = spmm_group_lanes(op);  // no sliced copy: direct kernel
   }
   switch (g) {
     case 4: launch_vec<VT, XT, LD, 4>(ex, op, vals, x, y, ep, stop); break;
@@ -1005,17 +1272,17 @@ struct TuneKey {
   const void* indptr;
   const void* indices;
   int64_t n, nnz;
-  int ld, vbytes, xbytes, tiled, panel;
+  int ld, vbytes, xbytes, tiled, panel, sell;
   bool operator<(const TuneKey& o) const {
-    return std::tie(device, indptr, indices, n, nnz, ld, vbytes, xbytes, tiled, panel) <
-           std::tie(o.device, o.indptr, o.indices, o.n, o.nnz, o.ld, o.vbytes, o.xbytes, o.tiled, o.panel);
+    return std::tie(device, indptr, indices, n, nnz, ld, vbytes, xbytes, tiled, panel, sell) <
+           std::tie(o.device, o.indptr, o.indices, o.n, o.nnz, o.ld, o.vbytes, o.xbytes, o.tiled, o.panel, o.sell);
   }
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, int> g_tune;
 
 // Kernel override for tuning and tests: SPECTRAL_INIT_SPMM_KERNEL = vec4 | vec8 |
-// vec16 | vec32 | tiled4 | tiled8 | gather4 | gather8 (unset or "auto": the
+// vec16 | vec32 | tiled4 | tiled8 | gather4 | gather8 | panel | sell | sell_l1 (unset or "auto": the
 // autotuner).  A choice the operator or the types cannot use is ignored.
 template <class VT, class XT, int LD>
 int forced_choice(const OpDev& op, bool tiled) {
@@ -1025,12 +1292,13 @@ int forced_choice(const OpDev& op, bool tiled) {
   static const std::pair<const char*, int> names[] = {{"vec4", 4},     {"vec8", 8},       {"vec16", 16},
                                                       {"vec32", 32},   {"tiled4", 104},   {"tiled8", 108},
                                                       {"gather4", 204}, {"gather8", 208},
-                                                      {"panel", 300}};
+                                                      {"panel", 300},  {"sell", 400},    {"sell_l1", 401}};
   for (const auto& nm : names) {
     if (v != nm.first) continue;
     const int c = nm.second;
     if (c > 100 && c < 200 && !tiled) return 0;
     if (c == 300 && (op.panels == nullptr || op.panels->n_pblocks <= 0)) return 0;
+    if (c >= 400 && (op.panels == nullptr || !op.panels->sell_ok)) return 0;
     if (c > 200 && !(std::is_same<VT, float>::value && std::is_same<XT, float>::value && LD == 4 &&
                      op.gather_blocks != nullptr && op.n_gather_blocks > 0))
       return 0;
@@ -1044,8 +1312,9 @@ void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT
                 const int* stop) {
   const bool tiled = op.row_blocks != nullptr && op.n_blocks > 0;
   const bool panel = op.panels != nullptr && op.panels->n_pblocks > 0;
+  const bool sell = op.panels != nullptr && op.panels->sell_ok;
   const TuneKey key{ex.device, op.indptr, op.indices, op.n, op.nnz, LD, static_cast<int>(sizeof(VT)),
-                    static_cast<int>(sizeof(XT)), tiled ? 1 : 0, panel ? 1 : 0};
+                    static_cast<int>(sizeof(XT)), tiled ? 1 : 0, panel ? 1 : 0, sell ? 1 : 0};
   int g = forced_choice<VT, XT, LD>(op, tiled);
   if (g != 0) {
     launch_lanes<VT, XT, LD>(g, ex, op, vals, x, y, ep, stop);
@@ -1078,6 +1347,10 @@ void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT
         cands.push_back(208);
       }
       if (op.panels != nullptr && op.panels->n_pblocks > 0) cands.push_back(300);
+      if (sell) {
+        cands.push_back(400);
+        cands.push_back(401);
+      }
       for (int cand : cands) {
         launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
         SI_CUDA(cudaEventRecord(e0, ex.stream));
@@ -1135,6 +1408,8 @@ void make_row_blocks(const Exec& ex, const OpDev& op, RowBlocks& rb) {
   build(kGatherBlockNnz, rb.n_gblocks, rb.gstarts, rb.gptrs);
   build(kPanelBlockNnz, rb.n_pblocks, rb.pstarts, rb.pptrs);
   rb.windows.clear();
+  rb.sell.reset();
+  rb.sell_failed = false;
 }
 
 int spmm_group_lanes(const OpDev& op) {

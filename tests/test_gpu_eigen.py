@@ -288,19 +288,36 @@ def test_lobpcg_wide_blocks(gpu_ctx, nc, block, precision):
 
 
 @pytest.mark.parametrize("variant", ["task", "tile"])
-@pytest.mark.parametrize("small", ["warp", "cta"])
+@pytest.mark.parametrize("small", ["warp", "cta", "reg"])
 def test_lobpcg_kernel_variants_agree(gpu_ctx, monkeypatch, variant, small):
     """The 4-column LOBPCG iteration with either Gram kernel (task-split warps,
-    default; register-tiled, SPECTRAL_INIT_GRAM=tile) and either small step
-    (one warp in registers, default for up to 16 columns; one CTA,
-    SPECTRAL_INIT_SMALL_STEP=cta) converges to the dense eigenpairs."""
+    default; register-tiled, SPECTRAL_INIT_GRAM=tile) and each small step (one
+    warp with the Gram in shared memory, SPECTRAL_INIT_SMALL_STEP=warp; one
+    128-thread CTA, the default; one warp in registers, =reg) converges to the
+    dense eigenpairs."""
     import spectral_init_b200 as si
     if variant == "tile":
         monkeypatch.setenv("SPECTRAL_INIT_GRAM", "tile")
-    if small == "cta":
-        monkeypatch.setenv("SPECTRAL_INIT_SMALL_STEP", "cta")
+    monkeypatch.setenv("SPECTRAL_INIT_SMALL_STEP", small)
     lap = load_csr("blobs_connected_2000", "comp_b_laplacian.npz")
     cfg = si.SpectralInitConfig(force_level=1, tol=1e-10)
+    (vals, vecs), level = si.solve_eigenproblem_pub(lap, 2, 42, cfg, ctx=gpu_ctx)
+    w = np.linalg.eigvalsh(lap.toarray())[:3]
+    assert level == 1
+    assert np.all(np.abs(vals - w) < 1e-10), (vals, w)
+    assert O.max_eigenpair_residual(lap, vals, vecs) < 1e-9
+
+
+@pytest.mark.parametrize("kernel", ["sell", "sell_l1", "panel", "vec4", "tiled4"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_lobpcg_spmm_variants_agree(gpu_ctx, monkeypatch, kernel, precision):
+    """The LOBPCG solve (with its fused SpMM epilogues and the mixed-precision
+    f32 phase) with each SpMM kernel forced converges to the dense eigenpairs."""
+    import spectral_init_b200 as si
+    monkeypatch.setenv("SPECTRAL_INIT_SPMM_KERNEL", kernel)
+    lap = load_csr("blobs_connected_2000", "comp_b_laplacian.npz")
+    prec = si.Precision.MIXED if precision == "mixed" else si.Precision.FP64
+    cfg = si.SpectralInitConfig(force_level=1, tol=1e-10, precision=prec)
     (vals, vecs), level = si.solve_eigenproblem_pub(lap, 2, 42, cfg, ctx=gpu_ctx)
     w = np.linalg.eigvalsh(lap.toarray())[:3]
     assert level == 1
