@@ -188,7 +188,9 @@ def test_spmm_prepared_operator(gpu_ctx, width, prec):
     dt = np.float32 if prec == "f32" else np.float64
     x = torch.from_numpy(np.random.default_rng(12).standard_normal((n, width)).astype(dt)).cuda()
     ref_once = op.apply(x)
-    first = op.apply_prepared(x).clone()
+    first = op.apply_prepared(x)
+    gpu_ctx.synchronize()  # the planned call is queued on the library's stream
+    first = first.clone()
     y = None
     for _ in range(3):
         y = op.apply_prepared(x, y)
@@ -227,7 +229,9 @@ def test_spmm_sliced_variants(gpu_ctx, kernel, matrix, width, prec):
     os.environ["SPECTRAL_INIT_SPMM_KERNEL"] = kernel
     try:
         op = si.CsrOperator(a, diag=0.75, ctx=gpu_ctx, with_f32=(prec == "f32"))
-        y1 = op.apply_prepared(x).clone()
+        y1 = op.apply_prepared(x)
+        gpu_ctx.synchronize()  # the planned call is queued on the library's stream
+        y1 = y1.clone()
         y2 = op.apply_prepared(x)
         gpu_ctx.synchronize()
     finally:
