@@ -67,18 +67,23 @@ struct PanelWindows {
   DevBuf<int64_t> w0;
 };
 
-// Sliced-ELL copy of an operator for the sliced SpMM.  Rows are sorted by
-// length (longest first) inside windows of kSellSortRows consecutive rows and
-// cut into slices of 32; slot (s, j, r), at slice_ptr[s] + 32 j + r, holds
-// entry j of row perm[32 s + r] (plen[32 s + r] entries; slots past a row's
-// length hold index 0 and value 0, rows past n have perm = 0xffffffff).
-// Slice s is as wide as its longest row.
-constexpr int kSellSortRows = 256;
+// Sliced-ELL copy of an operator for the sliced SpMM.  Rows of up to
+// `long_min - 1` entries are sorted by length (longest first) inside windows
+// of kSellSortRows consecutive rows and cut into slices of 32; slot (s, j, r),
+// at slice_ptr[s] + 32 j + r, holds entry j of row perm[32 s + r]
+// (plen[32 s + r] entries; slots past a row's length hold index 0 and value 0,
+// lanes without a row have perm = 0xffffffff).  A slice is as wide as its
+// longest row.  Rows of long_min or more entries are listed in long_rows
+// (window order) and read from the CSR arrays by a whole warp each.
+constexpr int kSellSortRows = 4096;
+constexpr int kSellSortThreads = 1024;
+constexpr int kSellMaxShort = 1024;  // long_min never exceeds this + 1
 struct SellLayout {
-  int64_t n_slices = 0;
+  int64_t n_slices = 0, n_long = 0;
   uint64_t slots = 0;
+  int long_min = 0;
   DevBuf<uint64_t> slice_ptr;  // n_slices + 1
-  DevBuf<uint32_t> perm, plen, idx;
+  DevBuf<uint32_t> perm, plen, idx, long_rows;
   DevBuf<float> v32;
   DevBuf<double> v64;
 };

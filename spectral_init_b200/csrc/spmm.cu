@@ -972,36 +972,82 @@ bool launch_panel(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, 
 // Sliced SpMM.  One lane owns one row of a 32-row slice of the sliced-ELL copy
 // (SellLayout), so a warp's index and value loads are two coalesced 128-byte
 // requests per 32 entries, no lane waits on another's row bounds, and the row
-// sum needs no cross-lane reduction: per stored entry the warp issues about
-// half an instruction besides the gather and the FMAs (the CSR kernels issue
-// three).  Rows are sorted by length inside 256-row windows so a slice is
-// about as wide as its average row.  Persistent CTAs (one or two per SM) own
-// contiguous slice ranges balanced by slot count; with L1-cached gathers the
-// x rows a CTA's neighbourhood touches stay in the SM's L1 for graphs whose
-// node order keeps neighbours near (kNN graphs of clustered data, locality
-// orders).
+// sum needs no cross-lane reduction.  Rows are sorted by length inside
+// 4096-row windows, so a slice is about as wide as its average row; rows far
+// longer than the mean (hubs of kNN graphs) would make their slice that wide
+// and are instead read from the CSR arrays by a whole warp each.  Persistent
+// CTAs own contiguous slice ranges (balanced by slot count) and an equal share
+// of the long rows; inside a CTA warps take long rows first, then slices, from
+// shared counters.  With L1-cached gathers the x rows of a CTA's neighbourhood
+// stay in the SM's L1 for graphs whose node order keeps neighbours near (kNN
+// graphs of clustered data, locality orders).
 
-// Rank sort of each window of kSellSortRows rows by length (longest first,
-// ties by row): one CTA a window.
-__global__ void __launch_bounds__(kSellSortRows) k_sell_sort(int64_t n, int64_t n_pad,
-                                                              const uint64_t* __restrict__ indptr,
-                                                              uint32_t* __restrict__ perm,
-                                                              uint32_t* __restrict__ plen) {
-  __shared__ long long len_s[kSellSortRows];
-  const int i = threadIdx.x;
-  const int64_t row = static_cast<int64_t>(blockIdx.x) * kSellSortRows + i;
-  const long long len = row < n ? static_cast<long long>(indptr[row + 1] - indptr[row]) : -1;
-  len_s[i] = len;
+// Counting sort of each window of kSellSortRows rows by length (longest
+// first), short rows only; the window's long rows go to its segment of
+// `long_tmp` and their count to long_cnt[window].  Positions past the
+// window's short rows are empty lanes.
+__global__ void __launch_bounds__(kSellSortThreads) k_sell_sort(int64_t n, const uint64_t* __restrict__ indptr,
+                                                                 int long_min, uint32_t* __restrict__ perm,
+                                                                 uint32_t* __restrict__ plen,
+                                                                 uint32_t* __restrict__ long_tmp,
+                                                                 uint64_t* __restrict__ long_cnt) {
+  constexpr int R = kSellSortRows / kSellSortThreads;
+  __shared__ int hist[kSellMaxShort + 1];  // bin long_min - 1 - len: longest first
+  __shared__ int n_long, n_short;
+  const int nb = long_min;  // lengths 0 .. long_min - 1
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0;
+  if (threadIdx.x == 0) n_long = 0;
   __syncthreads();
-  int rank = 0;
-  for (int j = 0; j < kSellSortRows; ++j) {
-    const long long o = len_s[j];
-    rank += (o > len || (o == len && j < i)) ? 1 : 0;
+  const int64_t w0 = static_cast<int64_t>(blockIdx.x) * kSellSortRows;
+  int lens[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const int64_t row = w0 + threadIdx.x + q * kSellSortThreads;
+    lens[q] = -1;
+    if (row < n) {
+      const uint64_t len = indptr[row + 1] - indptr[row];
+      if (len >= static_cast<uint64_t>(long_min)) {
+        const int p = atomicAdd(&n_long, 1);
+        long_tmp[w0 + p] = static_cast<uint32_t>(row);
+      } else {
+        lens[q] = static_cast<int>(len);
+        atomicAdd(&hist[nb - 1 - lens[q]], 1);
+      }
+    }
   }
-  const int64_t pos = static_cast<int64_t>(blockIdx.x) * kSellSortRows + rank;
-  if (pos < n_pad) {
-    perm[pos] = row < n ? static_cast<uint32_t>(row) : 0xffffffffu;
-    plen[pos] = row < n ? static_cast<uint32_t>(len) : 0u;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int i = 0; i < nb; ++i) {
+      const int c = hist[i];
+      hist[i] = run;
+      run += c;
+    }
+    n_short = run;
+    long_cnt[blockIdx.x] = static_cast<uint64_t>(n_long);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    if (lens[q] >= 0) {
+      const int p = atomicAdd(&hist[nb - 1 - lens[q]], 1);
+      perm[w0 + p] = static_cast<uint32_t>(w0 + threadIdx.x + q * kSellSortThreads);
+      plen[w0 + p] = static_cast<uint32_t>(lens[q]);
+    }
+  }
+  for (int i = n_short + threadIdx.x; i < kSellSortRows; i += blockDim.x) {
+    perm[w0 + i] = 0xffffffffu;
+    plen[w0 + i] = 0u;
+  }
+}
+
+// Long rows of every window into one list (window order).
+__global__ void k_sell_long_compact(int64_t n_win, const uint32_t* __restrict__ long_tmp,
+                                    const uint64_t* __restrict__ long_ptr, uint32_t* __restrict__ long_rows) {
+  for (int64_t w = blockIdx.x; w < n_win; w += gridDim.x) {
+    const uint64_t b = long_ptr[w];
+    const int c = static_cast<int>(long_ptr[w + 1] - b);
+    for (int i = threadIdx.x; i < c; i += blockDim.x) long_rows[b + i] = long_tmp[w * kSellSortRows + i];
   }
 }
 
@@ -1084,32 +1130,63 @@ __device__ __forceinline__ int64_t sell_bound(const uint64_t* __restrict__ slice
   return lo;
 }
 
+struct SellArgs {
+  int64_t n_slices, n_long;
+  const uint64_t* slice_ptr;
+  const uint32_t* perm;
+  const uint32_t* plen;
+  const uint32_t* sidx;
+  const uint32_t* long_rows;
+  const uint64_t* indptr;  // CSR arrays, for the long rows
+  const uint32_t* indices;
+};
+
 template <class VT, class XT, int LD, int U, int NT, bool L1>
-__global__ void __launch_bounds__(NT, 1) k_spmm_sell(int64_t n_slices, const uint64_t* __restrict__ slice_ptr,
-                                                     const uint32_t* __restrict__ perm,
-                                                     const uint32_t* __restrict__ plen,
-                                                     const uint32_t* __restrict__ sidx, const VT* __restrict__ sval,
-                                                     double diag, const XT* __restrict__ x, XT* __restrict__ y,
-                                                     Epilogue<XT> ep, const int* __restrict__ stop) {
+__global__ void __launch_bounds__(NT, 1) k_spmm_sell(SellArgs a, const VT* __restrict__ sval,
+                                                     const VT* __restrict__ vals, double diag,
+                                                     const XT* __restrict__ x, XT* __restrict__ y, Epilogue<XT> ep,
+                                                     const int* __restrict__ stop) {
   if (stop != nullptr && *stop != 0) return;
-  constexpr int NW = NT / 32;
+  __shared__ long long next_long, next_slice;
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x / 32;
-  const uint64_t total = slice_ptr[n_slices];
-  const int64_t s_lo = blockIdx.x == 0 ? 0 : sell_bound(slice_ptr, n_slices, total * blockIdx.x / gridDim.x);
-  const int64_t s_hi = blockIdx.x + 1 == gridDim.x ? n_slices
-                                                    : sell_bound(slice_ptr, n_slices, total * (blockIdx.x + 1) / gridDim.x);
-  for (int64_t s = s_lo + warp; s < s_hi; s += NW) {
-    const uint64_t base = slice_ptr[s];
-    const int64_t w = static_cast<int64_t>((slice_ptr[s + 1] - base) / 32);
-    const uint32_t row = perm[s * 32 + lane];
-    const int64_t len = plen[s * 32 + lane];
-    const uint32_t* __restrict__ ip = sidx + base + lane;
+  const uint64_t total = a.slice_ptr[a.n_slices];
+  const int64_t s_lo = blockIdx.x == 0 ? 0 : sell_bound(a.slice_ptr, a.n_slices, total * blockIdx.x / gridDim.x);
+  const int64_t s_hi =
+      blockIdx.x + 1 == gridDim.x ? a.n_slices : sell_bound(a.slice_ptr, a.n_slices, total * (blockIdx.x + 1) / gridDim.x);
+  const int64_t l_lo = a.n_long * blockIdx.x / gridDim.x;
+  const int64_t l_hi = a.n_long * (blockIdx.x + 1) / gridDim.x;
+  if (threadIdx.x == 0) {
+    next_long = l_lo;
+    next_slice = s_lo;
+  }
+  __syncthreads();
+  // long rows: a warp each, straight from the CSR arrays
+  const GlobalStream<VT> src{a.indices, vals};
+  const bool writer = group_writer<LD, 32>(lane);
+  for (;;) {
+    long long i = 0;
+    if (lane == 0) i = atomicAdd(reinterpret_cast<unsigned long long*>(&next_long), 1ull);
+    i = __shfl_sync(0xffffffffu, i, 0);
+    if (i >= l_hi) break;
+    const int64_t row = a.long_rows[i];
+    spmm_row<VT, XT, LD, 32>(row, a.indptr[row], a.indptr[row + 1], src, diag, x, y, ep, lane, 0xffffffffu, writer);
+  }
+  // slices: a lane a row
+  for (;;) {
+    long long s = 0;
+    if (lane == 0) s = atomicAdd(reinterpret_cast<unsigned long long*>(&next_slice), 1ull);
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if (s >= s_hi) break;
+    const uint64_t base = a.slice_ptr[s];
+    const int w = static_cast<int>((a.slice_ptr[s + 1] - base) / 32);
+    const uint32_t row = a.perm[s * 32 + lane];
+    const int len = static_cast<int>(a.plen[s * 32 + lane]);
+    const uint32_t* __restrict__ ip = a.sidx + base + lane;
     const VT* __restrict__ vp = sval + base + lane;
     double acc[LD];
 #pragma unroll
     for (int c = 0; c < LD; ++c) acc[c] = 0.0;
-    for (int64_t j0 = 0; j0 < w; j0 += U, ip += 32 * U, vp += 32 * U) {
+    for (int j0 = 0; j0 < w; j0 += U, ip += 32 * U, vp += 32 * U) {
       uint32_t jj[U];
       double vv[U];
 #pragma unroll
@@ -1148,19 +1225,33 @@ __global__ void __launch_bounds__(NT, 1) k_spmm_sell(int64_t n_slices, const uin
 const SellLayout* sell_layout(const Exec& ex, const OpDev& op) {
   if (op.panels == nullptr || !op.panels->sell_ok || op.panels->sell_failed) return nullptr;
   if (op.panels->sell) return op.panels->sell.get();
-  if (op.n <= 0 || op.n >= int64_t(0xffffffff) || op.nnz >= (int64_t(1) << 32)) return nullptr;
+  if (op.n <= 0 || op.n >= int64_t(0xffffffff) - kSellSortRows || op.nnz >= (int64_t(1) << 32)) return nullptr;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   SI_CUDA(cudaStreamIsCapturing(ex.stream, &cs));
   if (cs != cudaStreamCaptureStatusNone) return nullptr;
   auto L = std::make_unique<SellLayout>();
-  L->n_slices = (op.n + 31) / 32;
-  const int64_t n_pad = L->n_slices * 32;
+  // rows of 4x the mean length or more (at least 128, at most kSellMaxShort+1) are long
+  const double mean = static_cast<double>(op.nnz) / static_cast<double>(op.n);
+  L->long_min = static_cast<int>(std::min<double>(kSellMaxShort + 1, std::max(128.0, std::ceil(4.0 * mean))));
   const int64_t n_win = (op.n + kSellSortRows - 1) / kSellSortRows;
+  const int64_t n_pad = n_win * kSellSortRows;
+  L->n_slices = n_pad / 32;
   L->perm.alloc(static_cast<size_t>(n_pad), ex.stream);
   L->plen.alloc(static_cast<size_t>(n_pad), ex.stream);
-  k_sell_sort<<<static_cast<unsigned>(n_win), kSellSortRows, 0, ex.stream>>>(op.n, n_pad, op.indptr, L->perm.get(),
-                                                                              L->plen.get());
+  DevBuf<uint32_t> long_tmp(static_cast<size_t>(n_pad), ex.stream);
+  DevBuf<uint64_t> long_cnt(static_cast<size_t>(n_win + 1), ex.stream);
+  long_cnt.zero();
+  k_sell_sort<<<static_cast<unsigned>(n_win), kSellSortThreads, 0, ex.stream>>>(
+      op.n, op.indptr, L->long_min, L->perm.get(), L->plen.get(), long_tmp.get(), long_cnt.get());
   SI_LAUNCH_CHECK();
+  DevBuf<uint64_t> long_ptr(static_cast<size_t>(n_win + 1), ex.stream);
+  L->n_long = static_cast<int64_t>(exclusive_scan_u64(ex, long_cnt.get(), long_ptr.get(), n_win));
+  L->long_rows.alloc(static_cast<size_t>(std::max<int64_t>(L->n_long, 1)), ex.stream);
+  if (L->n_long > 0) {
+    const int gl = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(n_win, int64_t(ex.sms) * 8)));
+    k_sell_long_compact<<<gl, 256, 0, ex.stream>>>(n_win, long_tmp.get(), long_ptr.get(), L->long_rows.get());
+    SI_LAUNCH_CHECK();
+  }
   DevBuf<uint64_t> cnt(static_cast<size_t>(L->n_slices + 1), ex.stream);
   const int g1 = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((L->n_slices + 256) / 256, int64_t(ex.sms) * 8)));
   k_sell_widths<<<g1, 256, 0, ex.stream>>>(L->n_slices, L->plen.get(), cnt.get());
@@ -1168,18 +1259,17 @@ const SellLayout* sell_layout(const Exec& ex, const OpDev& op) {
   L->slice_ptr.alloc(static_cast<size_t>(L->n_slices + 1), ex.stream);
   L->slots = exclusive_scan_u64(ex, cnt.get(), L->slice_ptr.get(), L->n_slices);
   // the copy must fit beside the solver's work buffers: at most a quarter of
-  // the free memory, and no more than twice the stored entries
+  // the free memory
   const size_t per_slot = 4 + (op.v32 ? 4 : 0) + (op.v64 ? 8 : 0);
   size_t free_b = 0, total_b = 0;
   SI_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  if (L->slots > 2 * static_cast<uint64_t>(std::max<int64_t>(op.nnz, 1)) + 32ull * L->n_slices ||
-      L->slots * per_slot > free_b / 4) {
+  if (L->slots * per_slot > free_b / 4) {
     op.panels->sell_failed = true;
     return nullptr;
   }
-  L->idx.alloc(static_cast<size_t>(L->slots), ex.stream);
-  if (op.v32) L->v32.alloc(static_cast<size_t>(L->slots), ex.stream);
-  if (op.v64) L->v64.alloc(static_cast<size_t>(L->slots), ex.stream);
+  L->idx.alloc(static_cast<size_t>(std::max<uint64_t>(L->slots, 1)), ex.stream);
+  if (op.v32) L->v32.alloc(static_cast<size_t>(std::max<uint64_t>(L->slots, 1)), ex.stream);
+  if (op.v64) L->v64.alloc(static_cast<size_t>(std::max<uint64_t>(L->slots, 1)), ex.stream);
   const int g2 = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((L->n_slices + 7) / 8, int64_t(ex.sms) * 16)));
   k_sell_fill<<<g2, 256, 0, ex.stream>>>(L->n_slices, L->slice_ptr.get(), L->perm.get(), L->plen.get(), op.indptr,
                                           op.indices, op.v32, op.v64, L->idx.get(), L->v32.get(), L->v64.get());
@@ -1213,18 +1303,19 @@ bool launch_sell(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, X
   if (sval == nullptr) return false;
   constexpr int NT = sell_threads<XT, LD>();
   constexpr int U = sell_unroll<XT, LD>();
-  static std::atomic<int> ready[128];
+  static std::atomic<int> resident[128];
   const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
-  if (ready[dev] == 0) {
+  if (resident[dev] == 0) {
     SI_CUDA(cudaFuncSetAttribute(k_spmm_sell<VT, XT, LD, U, NT, L1>,
                                  cudaFuncAttributePreferredSharedMemoryCarveout, 0));
-    ready[dev] = 1;
+    int per_sm = 0;
+    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmm_sell<VT, XT, LD, U, NT, L1>, NT, 0));
+    resident[dev] = std::max(per_sm, 1);
   }
-  const int per_sm = 2048 / NT;
-  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(L->n_slices, int64_t(ex.sms) * per_sm)));
-  k_spmm_sell<VT, XT, LD, U, NT, L1><<<grid, NT, 0, ex.stream>>>(L->n_slices, L->slice_ptr.get(), L->perm.get(),
-                                                                 L->plen.get(), L->idx.get(), sval, op.diag, x, y, ep,
-                                                                 stop);
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(L->n_slices, int64_t(ex.sms) * resident[dev])));
+  const SellArgs args{L->n_slices, L->n_long, L->slice_ptr.get(), L->perm.get(), L->plen.get(),
+                      L->idx.get(), L->long_rows.get(), op.indptr, op.indices};
+  k_spmm_sell<VT, XT, LD, U, NT, L1><<<grid, NT, 0, ex.stream>>>(args, sval, vals, op.diag, x, y, ep, stop);
   SI_LAUNCH_CHECK();
   return true;
 }
@@ -1299,7 +1390,7 @@ int forced_choice(const OpDev& op, bool tiled) {
     if (c > 100 && c < 200 && !tiled) return 0;
     if (c == 300 && (op.panels == nullptr || op.panels->n_pblocks <= 0)) return 0;
     if (c >= 400 && (op.panels == nullptr || !op.panels->sell_ok)) return 0;
-    if (c > 200 && !(std::is_same<VT, float>::value && std::is_same<XT, float>::value && LD == 4 &&
+    if (c > 200 && c < 300 && !(std::is_same<VT, float>::value && std::is_same<XT, float>::value && LD == 4 &&
                      op.gather_blocks != nullptr && op.n_gather_blocks > 0))
       return 0;
     return c;
