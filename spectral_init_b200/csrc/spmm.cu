@@ -1141,7 +1141,12 @@ struct SellArgs {
   const uint32_t* indices;
 };
 
-template <class VT, class XT, int LD, int U, int NT, bool L1>
+// Bulk prefetch of [p, p + bytes) into L2 (p and bytes multiples of 16).
+__device__ __forceinline__ void l2_prefetch_bulk(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+template <class VT, class XT, int LD, int U, int NT, bool L1, bool PF>
 __global__ void __launch_bounds__(NT, 1) k_spmm_sell(SellArgs a, const VT* __restrict__ sval,
                                                      const VT* __restrict__ vals, double diag,
                                                      const XT* __restrict__ x, XT* __restrict__ y, Epilogue<XT> ep,
@@ -1172,11 +1177,22 @@ __global__ void __launch_bounds__(NT, 1) k_spmm_sell(SellArgs a, const VT* __res
     spmm_row<VT, XT, LD, 32>(row, a.indptr[row], a.indptr[row + 1], src, diag, x, y, ep, lane, 0xffffffffu, writer);
   }
   // slices: a lane a row
+  constexpr int NW = NT / 32;
   for (;;) {
     long long s = 0;
     if (lane == 0) s = atomicAdd(reinterpret_cast<unsigned long long*>(&next_slice), 1ull);
     s = __shfl_sync(0xffffffffu, s, 0);
     if (s >= s_hi) break;
+    if (PF && lane == 0 && s + NW < s_hi) {
+      // the slice a warp of this CTA takes about NW slices from now: its
+      // index and value streams into L2 while this slice is computed
+      const uint64_t pb = a.slice_ptr[s + NW];
+      const uint64_t pc = a.slice_ptr[s + NW + 1] - pb;
+      if (pc > 0) {
+        l2_prefetch_bulk(a.sidx + pb, static_cast<uint32_t>(pc * sizeof(uint32_t)));
+        l2_prefetch_bulk(sval + pb, static_cast<uint32_t>(pc * sizeof(VT)));
+      }
+    }
     const uint64_t base = a.slice_ptr[s];
     const int w = static_cast<int>((a.slice_ptr[s + 1] - base) / 32);
     const uint32_t row = a.perm[s * 32 + lane];
@@ -1287,7 +1303,7 @@ constexpr int sell_unroll() {
   return (LD * sizeof(XT) <= 32) ? 4 : (LD * sizeof(XT) <= 64 ? 2 : 1);
 }
 
-template <class VT, class XT, int LD, bool L1>
+template <class VT, class XT, int LD, bool L1, bool PF>
 bool launch_sell(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                  const int* stop) {
   const SellLayout* L = sell_layout(ex, op);
@@ -1306,16 +1322,16 @@ bool launch_sell(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, X
   static std::atomic<int> resident[128];
   const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
   if (resident[dev] == 0) {
-    SI_CUDA(cudaFuncSetAttribute(k_spmm_sell<VT, XT, LD, U, NT, L1>,
+    SI_CUDA(cudaFuncSetAttribute(k_spmm_sell<VT, XT, LD, U, NT, L1, PF>,
                                  cudaFuncAttributePreferredSharedMemoryCarveout, 0));
     int per_sm = 0;
-    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmm_sell<VT, XT, LD, U, NT, L1>, NT, 0));
+    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmm_sell<VT, XT, LD, U, NT, L1, PF>, NT, 0));
     resident[dev] = std::max(per_sm, 1);
   }
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(L->n_slices, int64_t(ex.sms) * resident[dev])));
   const SellArgs args{L->n_slices, L->n_long, L->slice_ptr.get(), L->perm.get(), L->plen.get(),
                       L->idx.get(), L->long_rows.get(), op.indptr, op.indices};
-  k_spmm_sell<VT, XT, LD, U, NT, L1><<<grid, NT, 0, ex.stream>>>(args, sval, vals, op.diag, x, y, ep, stop);
+  k_spmm_sell<VT, XT, LD, U, NT, L1, PF><<<grid, NT, 0, ex.stream>>>(args, sval, vals, op.diag, x, y, ep, stop);
   SI_LAUNCH_CHECK();
   return true;
 }
@@ -1328,10 +1344,15 @@ void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const 
     if (launch_panel<VT, XT, LD>(ex, op, vals, x, y, ep, stop)) return;
     g = spmm_group_lanes(op);  // no windows (inside a capture before first use): direct kernel
   }
-  if (g == 400 || g == 401) {
-    if (g == 400 ? launch_sell<VT, XT, LD, false>(ex, op, vals, x, y, ep, stop)
-                 : launch_sell<VT, XT, LD, true>(ex, op, vals, x, y, ep, stop))
-      return;
+  if (g >= 400 && g <= 403) {
+    bool ok = false;
+    switch (g) {
+      case 400: ok = launch_sell<VT, XT, LD, false, false>(ex, op, vals, x, y, ep, stop); break;
+      case 401: ok = launch_sell<VT, XT, LD, true, false>(ex, op, vals, x, y, ep, stop); break;
+      case 402: ok = launch_sell<VT, XT, LD, false, true>(ex, op, vals, x, y, ep, stop); break;
+      default: ok = launch_sell<VT, XT, LD, true, true>(ex, op, vals, x, y, ep, stop); break;
+    }
+    if (ok) return;
     g = spmm_group_lanes(op);  // no sliced copy: direct kernel
   }
   switch (g) {
@@ -1373,7 +1394,8 @@ std::mutex g_tune_mu;
 std::map<TuneKey, int> g_tune;
 
 // Kernel override for tuning and tests: SPECTRAL_INIT_SPMM_KERNEL = vec4 | vec8 |
-// vec16 | vec32 | tiled4 | tiled8 | gather4 | gather8 | panel | sell | sell_l1 (unset or "auto": the
+// vec16 | vec32 | tiled4 | tiled8 | gather4 | gather8 | panel | sell | sell_l1 | sell_pf |
+// sell_l1_pf (unset or "auto": the
 // autotuner).  A choice the operator or the types cannot use is ignored.
 template <class VT, class XT, int LD>
 int forced_choice(const OpDev& op, bool tiled) {
@@ -1383,7 +1405,8 @@ int forced_choice(const OpDev& op, bool tiled) {
   static const std::pair<const char*, int> names[] = {{"vec4", 4},     {"vec8", 8},       {"vec16", 16},
                                                       {"vec32", 32},   {"tiled4", 104},   {"tiled8", 108},
                                                       {"gather4", 204}, {"gather8", 208},
-                                                      {"panel", 300},  {"sell", 400},    {"sell_l1", 401}};
+                                                      {"panel", 300},  {"sell", 400},    {"sell_l1", 401},
+                                                      {"sell_pf", 402}, {"sell_l1_pf", 403}};
   for (const auto& nm : names) {
     if (v != nm.first) continue;
     const int c = nm.second;
@@ -1438,10 +1461,8 @@ void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT
         cands.push_back(208);
       }
       if (op.panels != nullptr && op.panels->n_pblocks > 0) cands.push_back(300);
-      if (sell) {
-        cands.push_back(400);
-        cands.push_back(401);
-      }
+      if (sell)
+        for (int c = 400; c <= 403; ++c) cands.push_back(c);
       for (int cand : cands) {
         launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
         SI_CUDA(cudaEventRecord(e0, ex.stream));
