@@ -1083,7 +1083,8 @@ __global__ void k_sell_fill(int64_t n_slices, const uint64_t* __restrict__ slice
   }
 }
 
-// x row gather for the sliced kernel: L1-cached (.nc) or L2-only (.cg).
+// x row gather for the sliced kernel: L1-cached (.nc; measured faster on
+// every operator tried) or L2-only (.cg).
 template <class XT, int LD, bool L1>
 struct SellRowLoad;
 template <int LD, bool L1>
@@ -1146,7 +1147,7 @@ __device__ __forceinline__ void l2_prefetch_bulk(const void* p, uint32_t bytes) 
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-template <class VT, class XT, int LD, int U, int NT, bool L1, bool PF>
+template <class VT, class XT, int LD, int U, int NT, bool L1, bool PF, bool PIPE>
 __global__ void __launch_bounds__(NT, 1) k_spmm_sell(SellArgs a, const VT* __restrict__ sval,
                                                      const VT* __restrict__ vals, double diag,
                                                      const XT* __restrict__ x, XT* __restrict__ y, Epilogue<XT> ep,
@@ -1202,22 +1203,62 @@ __global__ void __launch_bounds__(NT, 1) k_spmm_sell(SellArgs a, const VT* __res
     double acc[LD];
 #pragma unroll
     for (int c = 0; c < LD; ++c) acc[c] = 0.0;
-    for (int j0 = 0; j0 < w; j0 += U, ip += 32 * U, vp += 32 * U) {
+    if constexpr (PIPE) {
+      // the next U positions' indices and values are loaded before this U's
+      // gathers, so the stream latency overlaps the gather latency
       uint32_t jj[U];
-      double vv[U];
+      VT vr[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const bool ok = j0 + u < w;
+        const bool ok = u < w;
         jj[u] = ok ? ld_stream(ip + 32 * u) : 0u;
-        vv[u] = ok ? static_cast<double>(ld_stream(vp + 32 * u)) : 0.0;
+        vr[u] = ok ? ld_stream(vp + 32 * u) : VT(0);
       }
+      for (int j0 = 0; j0 < w; j0 += U) {
+        ip += 32 * U;
+        vp += 32 * U;
+        uint32_t nj[U];
+        VT nv[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (j0 + u < len) {
-          double xr[LD];
-          SellRowLoad<XT, LD, L1>::run(x + static_cast<size_t>(jj[u]) * LD, xr);
+        for (int u = 0; u < U; ++u) {
+          const bool ok = j0 + U + u < w;
+          nj[u] = ok ? ld_stream(ip + 32 * u) : 0u;
+          nv[u] = ok ? ld_stream(vp + 32 * u) : VT(0);
+        }
 #pragma unroll
-          for (int c = 0; c < LD; ++c) acc[c] = fma(vv[u], xr[c], acc[c]);
+        for (int u = 0; u < U; ++u) {
+          if (j0 + u < len) {
+            double xr[LD];
+            SellRowLoad<XT, LD, L1>::run(x + static_cast<size_t>(jj[u]) * LD, xr);
+            const double v = static_cast<double>(vr[u]);
+#pragma unroll
+            for (int c = 0; c < LD; ++c) acc[c] = fma(v, xr[c], acc[c]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          jj[u] = nj[u];
+          vr[u] = nv[u];
+        }
+      }
+    } else {
+      for (int j0 = 0; j0 < w; j0 += U, ip += 32 * U, vp += 32 * U) {
+        uint32_t jj[U];
+        double vv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const bool ok = j0 + u < w;
+          jj[u] = ok ? ld_stream(ip + 32 * u) : 0u;
+          vv[u] = ok ? static_cast<double>(ld_stream(vp + 32 * u)) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (j0 + u < len) {
+            double xr[LD];
+            SellRowLoad<XT, LD, L1>::run(x + static_cast<size_t>(jj[u]) * LD, xr);
+#pragma unroll
+            for (int c = 0; c < LD; ++c) acc[c] = fma(vv[u], xr[c], acc[c]);
+          }
         }
       }
     }
@@ -1303,7 +1344,7 @@ constexpr int sell_unroll() {
   return (LD * sizeof(XT) <= 32) ? 4 : (LD * sizeof(XT) <= 64 ? 2 : 1);
 }
 
-template <class VT, class XT, int LD, bool L1, bool PF>
+template <class VT, class XT, int LD, bool L1, bool PF, bool PIPE>
 bool launch_sell(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                  const int* stop) {
   const SellLayout* L = sell_layout(ex, op);
@@ -1322,16 +1363,16 @@ bool launch_sell(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, X
   static std::atomic<int> resident[128];
   const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
   if (resident[dev] == 0) {
-    SI_CUDA(cudaFuncSetAttribute(k_spmm_sell<VT, XT, LD, U, NT, L1, PF>,
+    SI_CUDA(cudaFuncSetAttribute(k_spmm_sell<VT, XT, LD, U, NT, L1, PF, PIPE>,
                                  cudaFuncAttributePreferredSharedMemoryCarveout, 0));
     int per_sm = 0;
-    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmm_sell<VT, XT, LD, U, NT, L1, PF>, NT, 0));
+    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmm_sell<VT, XT, LD, U, NT, L1, PF, PIPE>, NT, 0));
     resident[dev] = std::max(per_sm, 1);
   }
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(L->n_slices, int64_t(ex.sms) * resident[dev])));
   const SellArgs args{L->n_slices, L->n_long, L->slice_ptr.get(), L->perm.get(), L->plen.get(),
                       L->idx.get(), L->long_rows.get(), op.indptr, op.indices};
-  k_spmm_sell<VT, XT, LD, U, NT, L1, PF><<<grid, NT, 0, ex.stream>>>(args, sval, vals, op.diag, x, y, ep, stop);
+  k_spmm_sell<VT, XT, LD, U, NT, L1, PF, PIPE><<<grid, NT, 0, ex.stream>>>(args, sval, vals, op.diag, x, y, ep, stop);
   SI_LAUNCH_CHECK();
   return true;
 }
@@ -1347,10 +1388,10 @@ void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const 
   if (g >= 400 && g <= 403) {
     bool ok = false;
     switch (g) {
-      case 400: ok = launch_sell<VT, XT, LD, false, false>(ex, op, vals, x, y, ep, stop); break;
-      case 401: ok = launch_sell<VT, XT, LD, true, false>(ex, op, vals, x, y, ep, stop); break;
-      case 402: ok = launch_sell<VT, XT, LD, false, true>(ex, op, vals, x, y, ep, stop); break;
-      default: ok = launch_sell<VT, XT, LD, true, true>(ex, op, vals, x, y, ep, stop); break;
+      case 400: ok = launch_sell<VT, XT, LD, true, false, false>(ex, op, vals, x, y, ep, stop); break;
+      case 401: ok = launch_sell<VT, XT, LD, true, true, false>(ex, op, vals, x, y, ep, stop); break;
+      case 402: ok = launch_sell<VT, XT, LD, true, false, true>(ex, op, vals, x, y, ep, stop); break;
+      default: ok = launch_sell<VT, XT, LD, true, true, true>(ex, op, vals, x, y, ep, stop); break;
     }
     if (ok) return;
     g = spmm_group_lanes(op);  // no sliced copy: direct kernel
@@ -1394,8 +1435,8 @@ std::mutex g_tune_mu;
 std::map<TuneKey, int> g_tune;
 
 // Kernel override for tuning and tests: SPECTRAL_INIT_SPMM_KERNEL = vec4 | vec8 |
-// vec16 | vec32 | tiled4 | tiled8 | gather4 | gather8 | panel | sell | sell_l1 | sell_pf |
-// sell_l1_pf (unset or "auto": the
+// vec16 | vec32 | tiled4 | tiled8 | gather4 | gather8 | panel | sell | sell_pf | sell_pipe |
+// sell_pf_pipe (unset or "auto": the
 // autotuner).  A choice the operator or the types cannot use is ignored.
 template <class VT, class XT, int LD>
 int forced_choice(const OpDev& op, bool tiled) {
@@ -1405,8 +1446,8 @@ int forced_choice(const OpDev& op, bool tiled) {
   static const std::pair<const char*, int> names[] = {{"vec4", 4},     {"vec8", 8},       {"vec16", 16},
                                                       {"vec32", 32},   {"tiled4", 104},   {"tiled8", 108},
                                                       {"gather4", 204}, {"gather8", 208},
-                                                      {"panel", 300},  {"sell", 400},    {"sell_l1", 401},
-                                                      {"sell_pf", 402}, {"sell_l1_pf", 403}};
+                                                      {"panel", 300},  {"sell", 400},    {"sell_pf", 401},
+                                                      {"sell_pipe", 402}, {"sell_pf_pipe", 403}};
   for (const auto& nm : names) {
     if (v != nm.first) continue;
     const int c = nm.second;
