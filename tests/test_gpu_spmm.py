@@ -245,3 +245,28 @@ def test_spmm_sliced_variants(gpu_ctx, kernel, matrix, width, prec):
     xh = x.cpu().numpy().astype(np.float64)
     assert _rel(y1.cpu().numpy(), 0.75 * xh + av @ xh) < (2e-6 if prec == "f32" else 1e-14)
     op.close()
+
+
+def test_spmm_tuning_file(gpu_ctx, monkeypatch, tmp_path):
+    """SPECTRAL_INIT_SPMM_TUNE_FILE: the autotuner appends the choice it timed,
+    keyed by the operator's shape (n, nnz, width, value and block types)."""
+    import torch
+    import spectral_init_b200 as si
+    path = tmp_path / "tune.txt"
+    monkeypatch.setenv("SPECTRAL_INIT_SPMM_TUNE_FILE", str(path))
+    monkeypatch.delenv("SPECTRAL_INIT_SPMM_KERNEL", raising=False)
+    rng = np.random.default_rng(21)
+    n = 25_013  # a shape no other test uses
+    a = sp.random(n, n, density=12.0 / n, random_state=rng, format="csr")
+    a = (a + a.T).tocsr()
+    a.sort_indices()
+    op = si.CsrOperator(a, diag=1.0, ctx=gpu_ctx)
+    x = torch.from_numpy(rng.standard_normal((n, 4))).cuda()
+    y = op.apply_prepared(x)
+    gpu_ctx.synchronize()
+    xh = x.cpu().numpy()
+    assert _rel(y.cpu().numpy(), xh + a @ xh) < 1e-14
+    lines = [l.split() for l in path.read_text().splitlines()]
+    mine = [l for l in lines if int(l[0]) == n and int(l[1]) == a.nnz]
+    assert mine and all(len(l) == 9 and int(l[2]) == 4 and int(l[3]) == 8 and int(l[4]) == 8 for l in mine)
+    op.close()
