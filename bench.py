@@ -70,6 +70,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
+    p.add_argument("--block-size", type=int, default=0,
+                   help="LOBPCG block width (wanted pairs plus guard vectors; 0: the solver's choice)")
     p.add_argument("--spmm-profile", action="store_true", help="SpMM launches only (n=--n), for ncu")
     p.add_argument("--spmm-prec", choices=["both", "f64", "f32"], default="both",
                    help="with --spmm-profile: which SpMM precision to run")
@@ -331,6 +333,7 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         cfg.tol = tol
         cfg.mixed_switch_tol = a.switch_tol if switch_tol is None else switch_tol
         cfg.learned_filter = a.learned_filter if learned_filter is None else learned_filter
+        cfg.block_size = a.block_size
         vals = (C.c_double * k)()
         vecs = torch.empty(n, k, dtype=torch.float64, device=dev)
         level = C.c_int32(-1)
