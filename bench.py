@@ -353,8 +353,9 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         for name, prec, warm, tol in legs:
             solve(prec, warm, tol)
             ms, vals, _, level, rep = solve(prec, warm, tol)
-            out[name] = {"ms": ms, "iterations": rep.iterations, "level": level, "max_residual": rep.max_residual,
-                         "learned_start": rep.learned_start}
+            out[name] = {"ms": ms, "iterations": rep.iterations, "fp32_iterations": rep.fp32_iterations,
+                         "restarts": rep.restarts, "spmm_calls": rep.spmm_calls, "level": level,
+                         "max_residual": rep.max_residual, "learned_start": rep.learned_start}
         print(json.dumps({"profile_solve": True, "n": n, "nnz": nnz, **out}))
         return
 

@@ -1480,7 +1480,10 @@ void tune_file_append(const TuneKey& k, int choice) {  // caller holds g_tune_mu
 // autotuner).  A choice the operator or the types cannot use is ignored.
 template <class VT, class XT, int LD>
 int forced_choice(const OpDev& op, bool tiled) {
-  const char* env = std::getenv("SPECTRAL_INIT_SPMM_KERNEL");
+  // SPECTRAL_INIT_SPMM_KERNEL_F32 / _F64 override it for one value type
+  const char* env = std::getenv(std::is_same<VT, float>::value ? "SPECTRAL_INIT_SPMM_KERNEL_F32"
+                                                                : "SPECTRAL_INIT_SPMM_KERNEL_F64");
+  if (env == nullptr) env = std::getenv("SPECTRAL_INIT_SPMM_KERNEL");
   if (env == nullptr) return 0;
   const std::string v(env);
   static const std::pair<const char*, int> names[] = {{"vec4", 4},     {"vec8", 8},       {"vec16", 16},
