@@ -70,6 +70,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
+    p.add_argument("--solve-seed", type=int, default=None, help="eigensolver seed (default: --seed)")
     p.add_argument("--block-size", type=int, default=0,
                    help="LOBPCG block width (wanted pairs plus guard vectors; 0: the solver's choice)")
     p.add_argument("--spmm-profile", action="store_true", help="SpMM launches only (n=--n), for ncu")
@@ -341,7 +342,8 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        st = lib.si_solve_eigenproblem(ctx.ptr, C.byref(op), a.nc, a.seed, sq.data_ptr(), C.byref(cfg), vals,
+        st = lib.si_solve_eigenproblem(ctx.ptr, C.byref(op), a.nc, a.seed if a.solve_seed is None else a.solve_seed,
+                                       sq.data_ptr(), C.byref(cfg), vals,
                                        vecs.data_ptr(), C.byref(level), C.byref(rep))
         e1.record(stream)
         e1.synchronize()
