@@ -325,8 +325,10 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         legs.append(("fp64_same_tol", 0, 0, a.tol))
     head = "learned" if model is not None else "mixed"
 
+    base_seed = a.seed if a.solve_seed is None else a.solve_seed
+
     def solve(precision: int, warm: int = 0, tol: float = 0.0, switch_tol: float | None = None,
-              learned_filter: int | None = None):
+              learned_filter: int | None = None, seed: int | None = None):
         cfg = SiConfig()
         lib.si_config_default(C.byref(cfg))
         cfg.precision = precision
@@ -342,7 +344,7 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        st = lib.si_solve_eigenproblem(ctx.ptr, C.byref(op), a.nc, a.seed if a.solve_seed is None else a.solve_seed,
+        st = lib.si_solve_eigenproblem(ctx.ptr, C.byref(op), a.nc, base_seed if seed is None else seed,
                                        sq.data_ptr(), C.byref(cfg), vals,
                                        vecs.data_ptr(), C.byref(level), C.byref(rep))
         e1.record(stream)
@@ -399,22 +401,27 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
                           "oracle": None if oracle is None else oracle["summary"]}))
         return
 
+    # every leg solves the same seeds, one per timed step: LOBPCG's iteration
+    # count varies by tens of percent with the random start, so a single seed
+    # would rank the legs by luck
+    step_seeds = [base_seed + i for i in range(a.steps)]
     results = {}
     clocks = None
     launches_per_step = None
     for name, prec, warm, tol in legs:
-        for _ in range(a.warmup):
-            solve(prec, warm, tol)
+        for w in range(a.warmup):
+            solve(prec, warm, tol, seed=base_seed + 1000 + w)
         barrier()
         torch.cuda.synchronize()
         sampler = ClockSampler(local) if name == head else None
         if sampler:
             sampler.start()
         l0 = lib.si_kernel_launches()
-        times, last = [], None
-        for _ in range(a.steps):
-            ms, vals, vecs, level, rep = solve(prec, warm, tol)
+        times, iters, last = [], [], None
+        for sd in step_seeds:
+            ms, vals, vecs, level, rep = solve(prec, warm, tol, seed=sd)
             times.append(ms)
+            iters.append(rep.iterations)
             last = (vals, vecs, level, rep)
         torch.cuda.synchronize()
         barrier()
@@ -423,7 +430,9 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
             launches_per_step = (lib.si_kernel_launches() - l0) / a.steps
         ms_mean = max_over_ranks(statistics.mean(times))
         vals, vecs, level, rep = last
-        results[name] = {"ms": ms_mean, "ms_all": times, "tol": tol if tol > 0 else 1e-5, "eigenvalues": vals,
+        results[name] = {"ms": ms_mean, "ms_all": times, "iterations_all": iters,
+                         "iterations_mean": statistics.mean(iters), "tol": tol if tol > 0 else 1e-5,
+                         "eigenvalues": vals,
                          "level": level, "iterations": rep.iterations, "fp32_iterations": rep.fp32_iterations,
                          "restarts": rep.restarts, "max_residual": rep.max_residual,
                          "learned_start": rep.learned_start, "vecs": vecs}
@@ -456,16 +465,16 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         cfg.tol = a.tol
         rep = SiReport()
 
-        def call():
+        def call(sd):
             t = time.perf_counter()
-            ctx.check(lib.si_spectral_init(ctx.ptr, C.byref(hg), a.nc, a.seed, None, 0, C.byref(cfg),
+            ctx.check(lib.si_spectral_init(ctx.ptr, C.byref(hg), a.nc, sd, None, 0, C.byref(cfg),
                                            h_out.data_ptr(), C.byref(rep)))
             return time.perf_counter() - t
 
-        for _ in range(max(1, min(a.warmup, 2))):
-            call()
+        for w in range(max(1, min(a.warmup, 2))):
+            call(base_seed + 1000 + w)
         barrier()
-        ts = [call() for _ in range(a.steps)]
+        ts = [call(sd) for sd in step_seeds]
         barrier()
         e2e = {"value": max_over_ranks(statistics.mean(ts)), "unit": "s",
                "h2d_bytes_per_step": (n + 1) * 8 + nnz * 8, "d2h_bytes_per_step": n * a.nc * 4,
@@ -512,7 +521,7 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
                    f"{(nnz * 12 + (n + 1) * 8) / 1e6:.0f} MB f64 / {(nnz * 8 + (n + 1) * 8) / 1e6:.0f} MB f32)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "graph_build_s": round(t_gen, 2),
-                   "tol_value_leg": a.tol, "tol_fp64_leg": 1e-5,
+                   "tol_value_leg": a.tol, "tol_fp64_leg": 1e-5, "solve_seeds": step_seeds,
                    "warm_start": ("learned (committed network weights, trained on the n=10k-200k family)"
                                   + (", Chebyshev-filtered" if a.learned_filter else "")
                                   if head == "learned" else "random (no network weights found)")},
@@ -612,9 +621,11 @@ def run_reference(a):
     indptr, indices, data = make_graph(a, dev, 0)
     n = a.n
     op, sqh = CB.laplacian_operator(indptr.cpu().numpy(), indices.cpu().numpy(), data.cpu().numpy(), n)
-    for _ in range(a.warmup):
-        CB.solve_timed(op, a.nc, a.seed, sqh, budget_s=1.0)
-    samples = [CB.solve_measured(op, a.nc, a.seed, sqh) for _ in range(a.steps)]
+    base_seed = a.seed if a.solve_seed is None else a.solve_seed
+    for w in range(a.warmup):
+        CB.solve_timed(op, a.nc, base_seed + 1000 + w, sqh, budget_s=1.0)
+    # one solve seed per step, the seeds the GPU arm uses
+    samples = [CB.solve_measured(op, a.nc, base_seed + i, sqh) for i in range(a.steps)]
     val = statistics.mean(s["seconds"] for s in samples)
     s0 = samples[-1]
     conv = all(x["converged"] for x in samples)
@@ -623,7 +634,8 @@ def run_reference(a):
                       f"measured to {'convergence' if conv else 'its end'}: "
                       f"{s0['iterations']} iterations, max residual {s0['max_residual']:.2e}"),
            "iterations": s0["iterations"], "restarts": s0["restarts"], "converged": conv,
-           "seconds_all": [x["seconds"] for x in samples]}
+           "seconds_all": [x["seconds"] for x in samples], "iterations_all": [x["iterations"] for x in samples],
+           "solve_seeds": [base_seed + i for i in range(a.steps)]}
     line = {"metric": METRIC, "value": val, "unit": "s", "higher_is_better": False, "impl": "reference",
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": val * 1e3, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
