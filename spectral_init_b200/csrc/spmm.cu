@@ -1345,7 +1345,7 @@ constexpr int sell_unroll() {
   return (LD * sizeof(XT) <= 32) ? 4 : (LD * sizeof(XT) <= 64 ? 2 : 1);
 }
 
-template <class VT, class XT, int LD, bool L1, bool PF, bool PIPE, bool WIDE = false>
+template <class VT, class XT, int LD, bool L1, bool PF, bool PIPE>
 bool launch_sell(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
                  const int* stop) {
   const SellLayout* L = sell_layout(ex, op);
@@ -1359,9 +1359,7 @@ bool launch_sell(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, X
     sval = L->v64.get();
   }
   if (sval == nullptr) return false;
-  // WIDE: 1024 threads (64 registers) also for 32-byte rows, twice the warps
-  // of the default 512 at the cost of a few spilled registers
-  constexpr int NT = WIDE ? 1024 : sell_threads<XT, LD>();
+  constexpr int NT = sell_threads<XT, LD>();
   constexpr int U = sell_unroll<XT, LD>();
   static std::atomic<int> resident[128];
   const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
@@ -1388,16 +1386,13 @@ void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const 
     if (launch_panel<VT, XT, LD>(ex, op, vals, x, y, ep, stop)) return;
     g = spmm_group_lanes(op);  // no windows (inside a capture before first use): direct kernel
   }
-  if (g >= 400 && g <= 405) {
+  if (g >= 400 && g <= 403) {
     bool ok = false;
-    constexpr bool wide_differs = sell_threads<XT, LD>() < 1024 && LD * sizeof(XT) <= 32;
     switch (g) {
       case 400: ok = launch_sell<VT, XT, LD, true, false, false>(ex, op, vals, x, y, ep, stop); break;
       case 401: ok = launch_sell<VT, XT, LD, true, true, false>(ex, op, vals, x, y, ep, stop); break;
       case 402: ok = launch_sell<VT, XT, LD, true, false, true>(ex, op, vals, x, y, ep, stop); break;
-      case 403: ok = launch_sell<VT, XT, LD, true, true, true>(ex, op, vals, x, y, ep, stop); break;
-      case 404: ok = launch_sell<VT, XT, LD, true, false, false, wide_differs>(ex, op, vals, x, y, ep, stop); break;
-      default: ok = launch_sell<VT, XT, LD, true, false, true, wide_differs>(ex, op, vals, x, y, ep, stop); break;
+      default: ok = launch_sell<VT, XT, LD, true, true, true>(ex, op, vals, x, y, ep, stop); break;
     }
     if (ok) return;
     g = spmm_group_lanes(op);  // no sliced copy: direct kernel
@@ -1481,7 +1476,7 @@ void tune_file_append(const TuneKey& k, int choice) {  // caller holds g_tune_mu
 
 // Kernel override for tuning and tests: SPECTRAL_INIT_SPMM_KERNEL = vec4 | vec8 |
 // vec16 | vec32 | tiled4 | tiled8 | gather4 | gather8 | panel | sell | sell_pf | sell_pipe |
-// sell_pf_pipe | sell_wide | sell_wide_pipe (unset or "auto": the
+// sell_pf_pipe (unset or "auto": the
 // autotuner).  A choice the operator or the types cannot use is ignored.
 template <class VT, class XT, int LD>
 int forced_choice(const OpDev& op, bool tiled) {
@@ -1495,8 +1490,7 @@ int forced_choice(const OpDev& op, bool tiled) {
                                                       {"vec32", 32},   {"tiled4", 104},   {"tiled8", 108},
                                                       {"gather4", 204}, {"gather8", 208},
                                                       {"panel", 300},  {"sell", 400},    {"sell_pf", 401},
-                                                      {"sell_pipe", 402}, {"sell_pf_pipe", 403},
-                                                      {"sell_wide", 404}, {"sell_wide_pipe", 405}};
+                                                      {"sell_pipe", 402}, {"sell_pf_pipe", 403}};
   for (const auto& nm : names) {
     if (v != nm.first) continue;
     const int c = nm.second;
@@ -1562,13 +1556,8 @@ void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT
         cands.push_back(208);
       }
       if (op.panels != nullptr && op.panels->n_pblocks > 0) cands.push_back(300);
-      if (sell) {
+      if (sell)
         for (int c = 400; c <= 403; ++c) cands.push_back(c);
-        if (sell_threads<XT, LD>() < 1024 && LD * sizeof(XT) <= 32) {
-          cands.push_back(404);
-          cands.push_back(405);
-        }
-      }
       for (int cand : cands) {
         launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
         SI_CUDA(cudaEventRecord(e0, ex.stream));
