@@ -78,12 +78,7 @@ struct PanelWindows {
 constexpr int kSellSortRows = 4096;
 constexpr int kSellSortThreads = 1024;
 constexpr int kSellMaxShort = 1024;  // long_min never exceeds this + 1
-struct SellWindows {  // x window start per CTA of a `parts`-CTA launch (-1: none)
-  int W = 0, parts = 0;
-  DevBuf<int64_t> w0;
-};
 struct SellLayout {
-  mutable std::vector<SellWindows> windows;  // built on first use of each (W, parts)
   int64_t n_slices = 0, n_long = 0;
   uint64_t slots = 0;
   int long_min = 0;

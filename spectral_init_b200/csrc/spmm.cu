@@ -1133,8 +1133,7 @@ __device__ __forceinline__ int64_t sell_bound(const uint64_t* __restrict__ slice
 }
 
 struct SellArgs {
-  int64_t n, n_slices, n_long;
-  const int64_t* w0s;  // x window start per CTA (window kernels; -1: none)
+  int64_t n_slices, n_long;
   const uint64_t* slice_ptr;
   const uint32_t* perm;
   const uint32_t* plen;
@@ -1149,51 +1148,13 @@ __device__ __forceinline__ void l2_prefetch_bulk(const void* p, uint32_t bytes) 
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-__device__ __forceinline__ void cp_async_16(void* smem, const void* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-
-// Gather of one x row: from the shared-memory window [w0, w0 + wn) when the
-// kernel has one (WR > 0) and the row is inside, else from global memory.
-template <class XT, int LD, int WR>
-__device__ __forceinline__ void sell_gather(const XT* __restrict__ x, const XT* win, uint32_t j, uint32_t w0,
-                                            uint32_t wn, double (&xr)[LD]) {
-  if constexpr (WR > 0) {
-    const uint32_t d = j - w0;
-    if (d < wn) {
-      smem_row<XT, LD>(win + static_cast<size_t>(d) * LD, xr);
-      return;
-    }
-  }
-  SellRowLoad<XT, LD, true>::run(x + static_cast<size_t>(j) * LD, xr);
-}
-
-// WR > 0: each CTA first stages its x window (WR rows, chosen by the column
-// histogram of its rows) into shared memory with cp.async, computes its long
-// rows meanwhile (global gathers), then its slices with window gathers.
-template <class VT, class XT, int LD, int U, int NT, bool L1, bool PF, bool PIPE, int WR = 0>
+template <class VT, class XT, int LD, int U, int NT, bool L1, bool PF, bool PIPE>
 __global__ void __launch_bounds__(NT, 1) k_spmm_sell(SellArgs a, const VT* __restrict__ sval,
                                                      const VT* __restrict__ vals, double diag,
                                                      const XT* __restrict__ x, XT* __restrict__ y, Epilogue<XT> ep,
                                                      const int* __restrict__ stop) {
   if (stop != nullptr && *stop != 0) return;
-  extern __shared__ __align__(16) unsigned char sell_smem[];
-  const XT* win = reinterpret_cast<const XT*>(sell_smem);
   __shared__ long long next_long, next_slice;
-  uint32_t w0 = 0, wn = 0;
-  if constexpr (WR > 0) {
-    const int64_t ws = a.w0s[blockIdx.x];
-    if (ws >= 0) {
-      w0 = static_cast<uint32_t>(ws);
-      const int64_t rest = a.n - ws;
-      wn = static_cast<uint32_t>(rest < WR ? rest : WR);
-      const int chunks = static_cast<int>(static_cast<size_t>(wn) * LD * sizeof(XT) / 16);
-      const unsigned char* src = reinterpret_cast<const unsigned char*>(x + static_cast<size_t>(w0) * LD);
-      for (int c = threadIdx.x; c < chunks; c += NT) cp_async_16(sell_smem + 16 * c, src + 16 * c);
-      cp_async_commit_grp();
-    }
-  }
   const int lane = threadIdx.x & 31;
   const uint64_t total = a.slice_ptr[a.n_slices];
   const int64_t s_lo = blockIdx.x == 0 ? 0 : sell_bound(a.slice_ptr, a.n_slices, total * blockIdx.x / gridDim.x);
@@ -1216,10 +1177,6 @@ __global__ void __launch_bounds__(NT, 1) k_spmm_sell(SellArgs a, const VT* __res
     if (i >= l_hi) break;
     const int64_t row = a.long_rows[i];
     spmm_row<VT, XT, LD, 32>(row, a.indptr[row], a.indptr[row + 1], src, diag, x, y, ep, lane, 0xffffffffu, writer);
-  }
-  if constexpr (WR > 0) {
-    asm volatile("cp.async.wait_all;\n" ::);
-    __syncthreads();
   }
   // slices: a lane a row
   constexpr int NW = NT / 32;
@@ -1273,8 +1230,7 @@ __global__ void __launch_bounds__(NT, 1) k_spmm_sell(SellArgs a, const VT* __res
         for (int u = 0; u < U; ++u) {
           if (j0 + u < len) {
             double xr[LD];
-            if constexpr (WR > 0) sell_gather<XT, LD, WR>(x, win, jj[u], w0, wn, xr);
-            else SellRowLoad<XT, LD, L1>::run(x + static_cast<size_t>(jj[u]) * LD, xr);
+            SellRowLoad<XT, LD, L1>::run(x + static_cast<size_t>(jj[u]) * LD, xr);
             const double v = static_cast<double>(vr[u]);
 #pragma unroll
             for (int c = 0; c < LD; ++c) acc[c] = fma(v, xr[c], acc[c]);
@@ -1300,8 +1256,7 @@ __global__ void __launch_bounds__(NT, 1) k_spmm_sell(SellArgs a, const VT* __res
         for (int u = 0; u < U; ++u) {
           if (j0 + u < len) {
             double xr[LD];
-            if constexpr (WR > 0) sell_gather<XT, LD, WR>(x, win, jj[u], w0, wn, xr);
-            else SellRowLoad<XT, LD, L1>::run(x + static_cast<size_t>(jj[u]) * LD, xr);
+            SellRowLoad<XT, LD, L1>::run(x + static_cast<size_t>(jj[u]) * LD, xr);
 #pragma unroll
             for (int c = 0; c < LD; ++c) acc[c] = fma(vv[u], xr[c], acc[c]);
           }
@@ -1416,93 +1371,9 @@ bool launch_sell(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, X
     resident[dev] = std::max(per_sm, 1);
   }
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(L->n_slices, int64_t(ex.sms) * resident[dev])));
-  const SellArgs args{op.n,         L->n_slices,   L->n_long,          nullptr,   L->slice_ptr.get(),
-                      L->perm.get(), L->plen.get(), L->idx.get(),       L->long_rows.get(), op.indptr,
-                      op.indices};
+  const SellArgs args{L->n_slices, L->n_long, L->slice_ptr.get(), L->perm.get(), L->plen.get(),
+                      L->idx.get(), L->long_rows.get(), op.indptr, op.indices};
   k_spmm_sell<VT, XT, LD, U, NT, L1, PF, PIPE><<<grid, NT, 0, ex.stream>>>(args, sval, vals, op.diag, x, y, ep, stop);
-  SI_LAUNCH_CHECK();
-  return true;
-}
-
-// Row starts of the CTAs of a `parts`-CTA sliced launch (32 x each CTA's
-// first slice), the partition the kernel derives from slice_ptr.
-__global__ void k_sell_parts(const uint64_t* __restrict__ slice_ptr, int64_t n_slices, int parts, int64_t n,
-                             int64_t* __restrict__ prow) {
-  const uint64_t total = slice_ptr[n_slices];
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= parts; b += gridDim.x * blockDim.x) {
-    const int64_t s = b == 0 ? 0 : (b == parts ? n_slices : sell_bound(slice_ptr, n_slices, total * b / parts));
-    prow[b] = min(32 * s, n);
-  }
-}
-
-template <class XT, int LD>
-constexpr int sell_win_rows() {
-  return kPanelBytes / (LD * static_cast<int>(sizeof(XT)));
-}
-
-// x windows of the sliced kernel for `parts` CTAs of W rows (the panel plan
-// over each CTA's row range; built on first use outside stream capture).
-const int64_t* sell_windows(const Exec& ex, const OpDev& op, const SellLayout* L, int W, int parts) {
-  for (const SellWindows& sw : L->windows)
-    if (sw.W == W && sw.parts == parts) return sw.w0.get();
-  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  SI_CUDA(cudaStreamIsCapturing(ex.stream, &cs));
-  if (cs != cudaStreamCaptureStatusNone) return nullptr;
-  DevBuf<int64_t> prow(static_cast<size_t>(parts + 1), ex.stream);
-  k_sell_parts<<<(parts + 256) / 256, 256, 0, ex.stream>>>(L->slice_ptr.get(), L->n_slices, parts, op.n, prow.get());
-  SI_LAUNCH_CHECK();
-  int64_t bin = std::max<int64_t>(1, (W + 7) / 8);
-  int64_t nbins = (op.n + bin - 1) / bin;
-  if (nbins > kPanelBins) {
-    bin = (op.n + kPanelBins - 1) / kPanelBins;
-    nbins = (op.n + bin - 1) / bin;
-  }
-  SellWindows sw;
-  sw.W = W;
-  sw.parts = parts;
-  sw.w0.alloc(static_cast<size_t>(parts), ex.stream);
-  k_panel_windows<<<std::min(parts, ex.sms * 8), kPlanThreads, 0, ex.stream>>>(
-      op.n, op.indptr, op.indices, prow.get(), parts, W, static_cast<int>(bin),
-      static_cast<int>(std::max<int64_t>(nbins, 1)), sw.w0.get());
-  SI_LAUNCH_CHECK();
-  L->windows.push_back(std::move(sw));
-  return L->windows.back().w0.get();
-}
-
-// Sliced kernel with an x window in shared memory: one CTA per SM.
-template <class VT, class XT, int LD, bool PF, bool PIPE>
-bool launch_sell_win(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT* y, const Epilogue<XT>& ep,
-                     const int* stop) {
-  const SellLayout* L = sell_layout(ex, op);
-  if (L == nullptr || op.nnz >= (int64_t(1) << 32)) return false;
-  const VT* sval;
-  if constexpr (std::is_same<VT, float>::value) {
-    if (vals != op.v32) return false;
-    sval = L->v32.get();
-  } else {
-    if (vals != op.v64) return false;
-    sval = L->v64.get();
-  }
-  if (sval == nullptr) return false;
-  constexpr int NT = sell_threads<XT, LD>();
-  constexpr int U = sell_unroll<XT, LD>();
-  constexpr int WR = sell_win_rows<XT, LD>();
-  const int parts = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(L->n_slices, int64_t(ex.sms))));
-  const int64_t* w0s = sell_windows(ex, op, L, WR, parts);
-  if (w0s == nullptr) return false;
-  const int smem = WR * LD * static_cast<int>(sizeof(XT));
-  static std::atomic<int> ready[128];
-  const int dev = (ex.device >= 0 && ex.device < 128) ? ex.device : 0;
-  if (ready[dev] == 0) {
-    SI_CUDA(cudaFuncSetAttribute(k_spmm_sell<VT, XT, LD, U, NT, true, PF, PIPE, WR>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    ready[dev] = 1;
-  }
-  const SellArgs args{op.n,         L->n_slices,   L->n_long,    w0s,       L->slice_ptr.get(),
-                      L->perm.get(), L->plen.get(), L->idx.get(), L->long_rows.get(), op.indptr,
-                      op.indices};
-  k_spmm_sell<VT, XT, LD, U, NT, true, PF, PIPE, WR><<<parts, NT, smem, ex.stream>>>(args, sval, vals, op.diag, x, y,
-                                                                                      ep, stop);
   SI_LAUNCH_CHECK();
   return true;
 }
@@ -1514,16 +1385,6 @@ void launch_lanes(int g, const Exec& ex, const OpDev& op, const VT* vals, const 
   if (g == 300) {
     if (launch_panel<VT, XT, LD>(ex, op, vals, x, y, ep, stop)) return;
     g = spmm_group_lanes(op);  // no windows (inside a capture before first use): direct kernel
-  }
-  if (g >= 406 && g <= 408) {
-    bool ok = false;
-    switch (g) {
-      case 406: ok = launch_sell_win<VT, XT, LD, false, false>(ex, op, vals, x, y, ep, stop); break;
-      case 407: ok = launch_sell_win<VT, XT, LD, false, true>(ex, op, vals, x, y, ep, stop); break;
-      default: ok = launch_sell_win<VT, XT, LD, true, true>(ex, op, vals, x, y, ep, stop); break;
-    }
-    if (ok) return;
-    g = 400;  // no window plan (inside a capture before first use): the sliced kernel without one
   }
   if (g >= 400 && g <= 403) {
     bool ok = false;
@@ -1615,7 +1476,7 @@ void tune_file_append(const TuneKey& k, int choice) {  // caller holds g_tune_mu
 
 // Kernel override for tuning and tests: SPECTRAL_INIT_SPMM_KERNEL = vec4 | vec8 |
 // vec16 | vec32 | tiled4 | tiled8 | gather4 | gather8 | panel | sell | sell_pf | sell_pipe |
-// sell_pf_pipe | sell_win | sell_win_pipe | sell_win_pf_pipe (unset or "auto": the
+// sell_pf_pipe (unset or "auto": the
 // autotuner).  A choice the operator or the types cannot use is ignored.
 template <class VT, class XT, int LD>
 int forced_choice(const OpDev& op, bool tiled) {
@@ -1629,9 +1490,7 @@ int forced_choice(const OpDev& op, bool tiled) {
                                                       {"vec32", 32},   {"tiled4", 104},   {"tiled8", 108},
                                                       {"gather4", 204}, {"gather8", 208},
                                                       {"panel", 300},  {"sell", 400},    {"sell_pf", 401},
-                                                      {"sell_pipe", 402}, {"sell_pf_pipe", 403},
-                                                      {"sell_win", 406}, {"sell_win_pipe", 407},
-                                                      {"sell_win_pf_pipe", 408}};
+                                                      {"sell_pipe", 402}, {"sell_pf_pipe", 403}};
   for (const auto& nm : names) {
     if (v != nm.first) continue;
     const int c = nm.second;
@@ -1697,10 +1556,8 @@ void dispatch_g(const Exec& ex, const OpDev& op, const VT* vals, const XT* x, XT
         cands.push_back(208);
       }
       if (op.panels != nullptr && op.panels->n_pblocks > 0) cands.push_back(300);
-      if (sell) {
+      if (sell)
         for (int c = 400; c <= 403; ++c) cands.push_back(c);
-        for (int c = 406; c <= 408; ++c) cands.push_back(c);
-      }
       for (int cand : cands) {
         launch_lanes<VT, XT, LD>(cand, ex, op, vals, x, y, ep, nullptr);
         SI_CUDA(cudaEventRecord(e0, ex.stream));

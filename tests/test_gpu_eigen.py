@@ -308,7 +308,7 @@ def test_lobpcg_kernel_variants_agree(gpu_ctx, monkeypatch, variant, small):
     assert O.max_eigenpair_residual(lap, vals, vecs) < 1e-9
 
 
-@pytest.mark.parametrize("kernel", ["sell", "sell_pf_pipe", "sell_win_pipe", "panel", "vec4", "tiled4"])
+@pytest.mark.parametrize("kernel", ["sell", "sell_pf_pipe", "panel", "vec4", "tiled4"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_lobpcg_spmm_variants_agree(gpu_ctx, monkeypatch, kernel, precision):
     """The LOBPCG solve (with its fused SpMM epilogues and the mixed-precision

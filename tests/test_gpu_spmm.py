@@ -208,8 +208,7 @@ def test_spmm_prepared_operator(gpu_ctx, width, prec):
     op.close()
 
 
-@pytest.mark.parametrize("kernel", ["sell", "sell_pf", "sell_pipe", "sell_pf_pipe", "sell_win", "sell_win_pipe",
-                                    "sell_win_pf_pipe"])
+@pytest.mark.parametrize("kernel", ["sell", "sell_pf", "sell_pipe", "sell_pf_pipe"])
 @pytest.mark.parametrize("matrix", ["variant", "clustered"])
 @pytest.mark.parametrize("width", [4, 8, 16])
 @pytest.mark.parametrize("prec", ["f32", "f64"])
