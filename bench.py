@@ -417,11 +417,13 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         if sampler:
             sampler.start()
         l0 = lib.si_kernel_launches()
-        times, iters, last = [], [], None
+        times, iters, restarts, spmms, last = [], [], [], [], None
         for sd in step_seeds:
             ms, vals, vecs, level, rep = solve(prec, warm, tol, seed=sd)
             times.append(ms)
             iters.append(rep.iterations)
+            restarts.append(rep.restarts)
+            spmms.append(rep.spmm_calls)
             last = (vals, vecs, level, rep)
         torch.cuda.synchronize()
         barrier()
@@ -430,7 +432,8 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
             launches_per_step = (lib.si_kernel_launches() - l0) / a.steps
         ms_mean = max_over_ranks(statistics.mean(times))
         vals, vecs, level, rep = last
-        results[name] = {"ms": ms_mean, "ms_all": times, "iterations_all": iters,
+        results[name] = {"ms": ms_mean, "ms_all": times, "iterations_all": iters, "restarts_all": restarts,
+                         "spmm_calls_all": spmms,
                          "iterations_mean": statistics.mean(iters), "tol": tol if tol > 0 else 1e-5,
                          "eigenvalues": vals,
                          "level": level, "iterations": rep.iterations, "fp32_iterations": rep.fp32_iterations,
