@@ -71,6 +71,8 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
     p.add_argument("--solve-seed", type=int, default=None, help="eigensolver seed (default: --seed)")
+    p.add_argument("--profile-repeat", type=int, default=1,
+                   help="with --profile-solve: also time each leg this many times (same seed)")
     p.add_argument("--block-size", type=int, default=0,
                    help="LOBPCG block width (wanted pairs plus guard vectors; 0: the solver's choice)")
     p.add_argument("--spmm-profile", action="store_true", help="SpMM launches only (n=--n), for ncu")
@@ -356,6 +358,9 @@ def _run_ours_body(a, rank, world, local, dev, barrier, max_over_ranks):
         out = {}
         for name, prec, warm, tol in legs:
             solve(prec, warm, tol)
+            if a.profile_repeat > 1:
+                reps = [solve(prec, warm, tol) for _ in range(a.profile_repeat)]
+                out[name + "_repeat_ms"] = [round(r[0], 2) for r in reps]
             ms, vals, _, level, rep = solve(prec, warm, tol)
             out[name] = {"ms": ms, "iterations": rep.iterations, "fp32_iterations": rep.fp32_iterations,
                          "restarts": rep.restarts, "spmm_calls": rep.spmm_calls, "level": level,
