@@ -778,226 +778,10 @@ __device__ bool warp_rr_general(const double* gb, const double* ga, int P, const
   return true;
 }
 
-// ---------------------------------------------------------------------------
-// The generalised Rayleigh-Ritz for s <= 32 in one warp, on shared memory,
-// with a direct symmetric eigensolver instead of Jacobi sweeps.  Lane r owns
-// row r of every matrix (row stride LW = s rounded up to odd, so the lanes'
-// rows fall in distinct banks); __syncwarp orders the phases:
-//   * D-scaling to a unit-diagonal B, Cholesky B = L L^T (right-looking,
-//     lane r updates its own row);
-//   * Y = L^-1 A column by column (lane c forward-substitutes column c),
-//     C = Y L^-T row by row (lane r), then symmetrised;
-//   * Householder tridiagonalisation T = Q^T C Q (lane r updates row r of C
-//     and of Q; the reflector and its image through C go through shared
-//     vectors, the two dot products through warp sums);
-//   * the implicit QL iteration with Wilkinson shifts on T (Bowdler, Martin,
-//     Reinsch and Wilkinson, Numer. Math. 11, 1968, the EISPACK tql2
-//     method): every lane runs the same scalar recurrence on a private copy
-//     of the diagonal and off-diagonal and applies each plane rotation to
-//     its own row of Q, so the iteration needs no communication at all;
-//   * Z = D L^-T V_sel by back substitution, one lane per selected column.
-// Returns 1 on success, 0 when B is not positive definite (the caller's
-// breakdown handling, as for the Jacobi routine) and 2 when the QL iteration
-// did not converge (the caller then runs the Jacobi routine).
-constexpr int WQL = 32;
-constexpr int QL_MAXIT = 60;
-
-__device__ int warp_rr_ql(const double* gb, const double* ga, int P, const int* idx, int s, int nsel, int largest,
-                          double chol_tol, SmallSmem sm, double* theta_out) {
-  const int r = threadIdx.x & 31;
-  const int LW = s | 1;
-  double* Bm = sm.A;  // B, then L (lower triangle)
-  double* Am = sm.B;  // A, then Y, then C, then T
-  double* Qm = sm.V;  // Householder Q, then the eigenvectors of C
-  double* vec = sm.T;  // [0, 32) reflector, [32, 64) its image, [64, 96) D, [96, 128) 1 / L_ii
-  int* ord = reinterpret_cast<int*>(sm.T + 128);
-  const bool own = r < s;
-  // ---- load and D-scale ----------------------------------------------------
-  double dr = 1.0;
-  if (own) {
-    const int gi = idx[r];
-    for (int j = 0; j < s; ++j) {
-      const int gj = idx[j];
-      Bm[r * LW + j] = gb[gi * P + gj];
-      Am[r * LW + j] = ga[gi * P + gj];
-    }
-    dr = Bm[r * LW + r];
-  }
-  const bool badd = own && !(dr > 0.0 && isfinite(dr));
-  if (__any_sync(0xffffffffu, badd)) return 0;
-  const double dsr = own ? 1.0 / sqrt(dr) : 0.0;
-  vec[64 + r] = dsr;
-  __syncwarp();
-  if (own) {
-    for (int j = 0; j < s; ++j) {
-      const double f = dsr * vec[64 + j];
-      Bm[r * LW + j] *= f;
-      Am[r * LW + j] *= f;
-    }
-  }
-  __syncwarp();
-  // ---- Cholesky --------------------------------------------------------------
-  for (int j = 0; j < s; ++j) {
-    const double piv = Bm[j * LW + j];
-    if (!(piv > chol_tol)) return 0;  // every lane reads the same pivot
-    const double ljj = sqrt(piv);
-    const double inv = 1.0 / ljj;
-    if (r > j && own) Bm[r * LW + j] *= inv;
-    if (r == j) {
-      Bm[j * LW + j] = ljj;
-      vec[96 + j] = inv;
-    }
-    __syncwarp();
-    if (r > j && own) {
-      const double lrj = Bm[r * LW + j];
-      for (int k = j + 1; k <= r; ++k) Bm[r * LW + k] -= lrj * Bm[k * LW + j];
-    }
-    __syncwarp();
-  }
-  // ---- C = L^-1 A L^-T -------------------------------------------------------
-  if (own) {  // column r of Y = L^-1 A
-    for (int i = 0; i < s; ++i) {
-      double v = Am[i * LW + r];
-      for (int k = 0; k < i; ++k) v -= Bm[i * LW + k] * Am[k * LW + r];
-      Am[i * LW + r] = v * vec[96 + i];
-    }
-  }
-  __syncwarp();
-  if (own) {  // row r of C = Y L^-T
-    for (int j = 0; j < s; ++j) {
-      double v = Am[r * LW + j];
-      for (int k = 0; k < j; ++k) v -= Am[r * LW + k] * Bm[j * LW + k];
-      Am[r * LW + j] = v * vec[96 + j];
-    }
-  }
-  __syncwarp();
-  if (own) {
-    for (int j = r + 1; j < s; ++j) {
-      const double v = 0.5 * (Am[r * LW + j] + Am[j * LW + r]);
-      Am[r * LW + j] = v;
-      Am[j * LW + r] = v;
-    }
-    for (int j = 0; j < s; ++j) Qm[r * LW + j] = (j == r) ? 1.0 : 0.0;
-  }
-  __syncwarp();
-  // ---- Householder tridiagonalisation: C = Q T Q^T -----------------------------
-  for (int k = 0; k + 2 < s; ++k) {
-    const double x = (own && r > k) ? Am[r * LW + k] : 0.0;
-    const double sigma = warp_sum(x * x);
-    const double x1 = __shfl_sync(0xffffffffu, x, k + 1);
-    if (!(sigma > x1 * x1 * 1e-300) || sigma == x1 * x1) continue;  // column already reduced
-    const double alpha = -copysign(sqrt(sigma), x1);
-    const double vr = (r == k + 1) ? x - alpha : x;  // zero at and above row k
-    const double tau = 1.0 / (sigma - alpha * x1);   // 2 / (v^T v)
-    vec[r] = vr;
-    __syncwarp();
-    double p = 0.0;
-    if (own && r > k)
-      for (int j = k + 1; j < s; ++j) p += Am[r * LW + j] * vec[j];
-    const double vp = warp_sum(vr * p);
-    const double wr = tau * p - 0.5 * tau * tau * vp * vr;
-    vec[32 + r] = wr;
-    __syncwarp();
-    if (own && r > k) {
-      for (int j = k + 1; j < s; ++j) Am[r * LW + j] -= vr * vec[32 + j] + wr * vec[j];
-      const double sub = (r == k + 1) ? alpha : 0.0;
-      Am[r * LW + k] = sub;
-      Am[k * LW + r] = sub;
-    }
-    if (own) {
-      double qv = 0.0;
-      for (int j = k + 1; j < s; ++j) qv += Qm[r * LW + j] * vec[j];
-      qv *= tau;
-      for (int j = k + 1; j < s; ++j) Qm[r * LW + j] -= qv * vec[j];
-    }
-    __syncwarp();
-  }
-  // ---- implicit QL on the tridiagonal (private copy in every lane) ------------
-  double d[WQL], e[WQL];
-  for (int i = 0; i < s; ++i) {
-    d[i] = Am[i * LW + i];
-    e[i] = (i + 1 < s) ? Am[(i + 1) * LW + i] : 0.0;
-  }
-  double* qrow = Qm + (own ? r : 0) * LW;
-  bool conv = true;
-  for (int l = 0; l < s && conv; ++l) {
-    for (int it = 0;; ++it) {
-      int m = l;
-      while (m + 1 < s && fabs(e[m]) > DBL_EPSILON * (fabs(d[m]) + fabs(d[m + 1]))) ++m;
-      if (m == l) break;
-      if (it == QL_MAXIT) {
-        conv = false;
-        break;
-      }
-      // Wilkinson-type shift from the leading 2 x 2 block
-      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-      double h = hypot(g, 1.0);
-      g = d[m] - d[l] + e[l] / (g + copysign(h, g));
-      double sn = 1.0, cs = 1.0, shift = 0.0;
-      bool early = false;
-      for (int i = m - 1; i >= l; --i) {
-        const double f = sn * e[i];
-        const double b = cs * e[i];
-        h = hypot(f, g);
-        e[i + 1] = h;
-        if (h == 0.0) {  // the chase underflowed: deflate and restart the sweep
-          d[i + 1] -= shift;
-          e[m] = 0.0;
-          early = true;
-          break;
-        }
-        const double ih = 1.0 / h;
-        sn = f * ih;
-        cs = g * ih;
-        g = d[i + 1] - shift;
-        const double t = (d[i] - g) * sn + 2.0 * cs * b;
-        shift = sn * t;
-        d[i + 1] = g + shift;
-        g = cs * t - b;
-        if (own) {
-          const double qa = qrow[i], qb = qrow[i + 1];
-          qrow[i + 1] = sn * qa + cs * qb;
-          qrow[i] = cs * qa - sn * qb;
-        }
-      }
-      if (early) continue;
-      d[l] -= shift;
-      e[l] = g;
-      e[m] = 0.0;
-    }
-  }
-  if (!conv) return 2;
-  // ---- selection and Z = D L^-T V_sel -----------------------------------------
-  if (own) {  // rank of eigenvalue r (ascending, or descending for `largest`; ties by index)
-    int rank = 0;
-    for (int j = 0; j < s; ++j) {
-      const bool before = largest ? (d[j] > d[r] || (d[j] == d[r] && j < r)) : (d[j] < d[r] || (d[j] == d[r] && j < r));
-      rank += before ? 1 : 0;
-    }
-    ord[rank] = r;
-  }
-  __syncwarp();
-  if (r < nsel) {
-    const int c = ord[r];
-    theta_out[r] = d[c];
-    for (int i = s - 1; i >= 0; --i) {
-      double v = Qm[i * LW + c];
-      for (int k = i + 1; k < s; ++k) v -= Bm[k * LW + i] * sm.Z[k * sm.ld + r];
-      sm.Z[i * sm.ld + r] = v * vec[96 + i];
-    }
-    for (int i = 0; i < s; ++i) sm.Z[i * sm.ld + r] *= vec[64 + i];
-  }
-  __syncwarp();
-  return 1;
-}
-
-// Rayleigh-Ritz of the small step: with QL (the default) the one-warp
-// tridiagonal QL routine for problems up to 32 wide, the rest of the CTA
-// waiting at the barrier (the Jacobi routine runs if QL does not converge);
-// otherwise the shared-memory CTA routines (on a single-warp CTA their
-// barriers are warp-cheap), or, with REG, the register-resident warp version
-// (SPECTRAL_INIT_SMALL_STEP=reg).
-template <int NT, bool REG, bool QL>
+// Rayleigh-Ritz of the small step: the shared-memory CTA routines (on a
+// single-warp CTA their barriers are warp-cheap), or, with REG, the
+// register-resident warp version (SPECTRAL_INIT_SMALL_STEP=reg).
+template <int NT, bool REG>
 __device__ bool rr_general(const double* gb, const double* ga, int P, const int* idx, int s, int nsel, int largest,
                            double chol_tol, SmallSmem sm, double* dsc, double* theta_out, double* red, double* rc,
                            double* rs, int* ra, int* rb, int* order, int* sflag) {
@@ -1005,26 +789,12 @@ __device__ bool rr_general(const double* gb, const double* ga, int P, const int*
     if (s <= WRR)
       return warp_rr_general(gb, ga, P, idx, s, nsel, largest, chol_tol, sm.Z, sm.ld, sm.T, theta_out);
   }
-  if constexpr (QL) {
-    if (s <= WQL) {
-      __shared__ int ql_status;
-      if (threadIdx.x < 32) {
-        const int st = warp_rr_ql(gb, ga, P, idx, s, nsel, largest, chol_tol, sm, theta_out);
-        if (threadIdx.x == 0) ql_status = st;
-      }
-      __syncthreads();
-      const int st = ql_status;
-      __syncthreads();  // read by every thread before a later call rewrites it
-      if (st == 1) return true;
-      if (st == 0) return false;
-    }
-  }
   return cta_rr_general(gb, ga, P, idx, s, nsel, largest, chol_tol, sm, dsc, theta_out, red, rc, rs, ra, rb, order,
                         sflag);
 }
 
 // `ctrl` points to the CTA's shared-memory copy of the control block.
-template <int NT, bool REG, bool QL>
+template <int NT, bool REG>
 __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns, int mode,
                                 double* smem) {
   __shared__ double red[ST_WIDE / 32];
@@ -1048,7 +818,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
   if (mode == SM_INIT) {
     for (int i = threadIdx.x; i < m; i += blockDim.x) idx[i] = i;
     __syncthreads();
-    const bool ok = rr_general<NT, REG, QL>(gb, ga, P, idx, m, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc,
+    const bool ok = rr_general<NT, REG>(gb, ga, P, idx, m, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc,
                                    rs, ra, rb, order, &sflag);
     if (threadIdx.x == 0) {
       ctrl->iter = 0;
@@ -1173,12 +943,12 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
         if (ctrl->active[c]) idx[m + na + q++] = 2 * m + c;
     }
     __syncthreads();
-    ok = rr_general<NT, REG, QL>(gb, ga, P, idx, m + 2 * na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs,
+    ok = rr_general<NT, REG>(gb, ga, P, idx, m + 2 * na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs,
                         ra, rb, order, &sflag);
     if (!ok) withp = 0;
   }
   if (!ok) {
-    ok = rr_general<NT, REG, QL>(gb, ga, P, idx, m + na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs, ra,
+    ok = rr_general<NT, REG>(gb, ga, P, idx, m + na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs, ra,
                         rb, order, &sflag);
   }
   if (!ok) {
@@ -1215,7 +985,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
 
 // The control block is staged in shared memory for the whole step (the step
 // is a long chain of small dependent updates) and written back at the end.
-template <int NT, bool REG = false, bool QL = false>
+template <int NT, bool REG = false>
 __global__ void __launch_bounds__(NT, 1) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
                                                    int mode) {
   extern __shared__ double smem[];
@@ -1226,7 +996,7 @@ __global__ void __launch_bounds__(NT, 1) k_small_step(LobpcgCtrl* ctrl, const do
   const double* src = reinterpret_cast<const double*>(ctrl);
   for (int i = threadIdx.x; i < W; i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  small_step_body<NT, REG, QL>(&sctrl, gram, ns, mode, smem);
+  small_step_body<NT, REG>(&sctrl, gram, ns, mode, smem);
   __syncthreads();
   double* back = reinterpret_cast<double*>(ctrl);
   for (int i = threadIdx.x; i < W; i += blockDim.x) back[i] = dst[i];
@@ -1283,7 +1053,7 @@ int small_step_variant() {
   const char* e = std::getenv("SPECTRAL_INIT_SMALL_STEP");
   if (e == nullptr) return 1;
   const std::string v(e);
-  return v == "warp" ? 0 : (v == "reg" ? 2 : (v == "jacobi" ? 3 : 1));
+  return v == "warp" ? 0 : (v == "reg" ? 2 : 1);
 }
 
 void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode, int m) {
@@ -1295,10 +1065,6 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
                                  static_cast<int>(smem)));
     SI_CUDA(cudaFuncSetAttribute(k_small_step<ST_WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
-    SI_CUDA(cudaFuncSetAttribute(k_small_step<ST, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
-    SI_CUDA(cudaFuncSetAttribute(k_small_step<ST_WIDE, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
     SI_CUDA(cudaFuncSetAttribute(k_small_step<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
     SI_CUDA(cudaFuncSetAttribute(k_small_step<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1307,17 +1073,11 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
   }
   // the Rayleigh-Ritz problem has up to ns * m rows: up to 16 fit one warp's
   // registers; wider blocks get a CTA, the widest the most threads
-  // (SPECTRAL_INIT_SMALL_STEP: unset, the CTA with the one-warp QL
-  // Rayleigh-Ritz; jacobi, the CTA with Jacobi sweeps; warp / reg, one warp)
-  const int variant = small_step_variant();
-  const bool ql = variant == 1;
-  if (ns * m > 24) {
-    if (ql) k_small_step<ST_WIDE, false, true><<<1, ST_WIDE, smem, ex.stream>>>(ctrl, gram, ns, mode);
-    else k_small_step<ST_WIDE><<<1, ST_WIDE, smem, ex.stream>>>(ctrl, gram, ns, mode);
-  } else if (ns * m > WRR || variant == 1 || variant == 3) {
-    if (ql) k_small_step<ST, false, true><<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
-    else k_small_step<ST><<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
-  } else if (variant == 2)
+  if (ns * m > 24)
+    k_small_step<ST_WIDE><<<1, ST_WIDE, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  else if (ns * m > WRR || small_step_variant() == 1)
+    k_small_step<ST><<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  else if (small_step_variant() == 2)
     k_small_step<32, true><<<1, 32, smem, ex.stream>>>(ctrl, gram, ns, mode);
   else
     k_small_step<32><<<1, 32, smem, ex.stream>>>(ctrl, gram, ns, mode);

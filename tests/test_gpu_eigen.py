@@ -288,21 +288,17 @@ def test_lobpcg_wide_blocks(gpu_ctx, nc, block, precision):
 
 
 @pytest.mark.parametrize("variant", ["task", "tile"])
-@pytest.mark.parametrize("small", ["default", "jacobi", "warp", "reg"])
+@pytest.mark.parametrize("small", ["warp", "cta", "reg"])
 def test_lobpcg_kernel_variants_agree(gpu_ctx, monkeypatch, variant, small):
     """The 4-column LOBPCG iteration with either Gram kernel (task-split warps,
-    default; register-tiled, SPECTRAL_INIT_GRAM=tile) and each small step (the
-    128-thread CTA with the one-warp tridiagonal QL Rayleigh-Ritz, the default;
-    the same CTA with Jacobi sweeps, SPECTRAL_INIT_SMALL_STEP=jacobi; one warp
-    with the Gram in shared memory, =warp; one warp in registers, =reg)
-    converges to the dense eigenpairs."""
+    default; register-tiled, SPECTRAL_INIT_GRAM=tile) and each small step (one
+    warp with the Gram in shared memory, SPECTRAL_INIT_SMALL_STEP=warp; one
+    128-thread CTA, the default; one warp in registers, =reg) converges to the
+    dense eigenpairs."""
     import spectral_init_b200 as si
     if variant == "tile":
         monkeypatch.setenv("SPECTRAL_INIT_GRAM", "tile")
-    if small == "default":
-        monkeypatch.delenv("SPECTRAL_INIT_SMALL_STEP", raising=False)
-    else:
-        monkeypatch.setenv("SPECTRAL_INIT_SMALL_STEP", small)
+    monkeypatch.setenv("SPECTRAL_INIT_SMALL_STEP", small)
     lap = load_csr("blobs_connected_2000", "comp_b_laplacian.npz")
     cfg = si.SpectralInitConfig(force_level=1, tol=1e-10)
     (vals, vecs), level = si.solve_eigenproblem_pub(lap, 2, 42, cfg, ctx=gpu_ctx)
