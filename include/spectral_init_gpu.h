@@ -79,7 +79,7 @@ typedef struct si_config {
                                 LOBPCG_ACCEPT_TOL (src/metrics.rs:40).  Smaller values
                                 give more accurate pairs; the level-1/3 residual gate
                                 stays 1e-5 (src/metrics.rs:30)                       */
-  double mixed_switch_tol;   /* mixed mode: f32 phase stops at this residual; <=0 auto */
+  double mixed_switch_tol;   /* mixed mode: f32 phase stops at this residual; <=0 auto (1e-4, 1e-5 from a learned block) */
 } si_config;
 
 /* Per-call diagnostics. */
