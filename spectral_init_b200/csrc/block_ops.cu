@@ -686,300 +686,6 @@ __global__ void __launch_bounds__(256) k_lobpcg_update4(LobpcgBlocks<XT> b, cons
   }
 }
 
-// ---------------------------------------------------------------------------
-// Gram products folded into the 4-column LOBPCG update.  The next iteration's
-// Gram needs the upper triangles of S = [X R P]^T [X R P] and
-// G = [X R P]^T [AX AR AP] (78 + 78 entries, layout below).  The update
-// writes X, R, P, AX and AP, so it forms every entry whose second factor is
-// not AR (130 of 156) from the values it stores, while they are in
-// registers; only X^T AR and the upper triangle of R^T AR (26 entries) wait
-// for the SpMM that produces AR (k_gram_ar4, three blocks read instead of
-// six).  Both kernels write one 156-entry row per CTA (zeros where they own
-// nothing) and k_gram156_reduce adds the rows in CTA order: deterministic.
-// Entry e < 78: S(i, j), e >= 78: G(i, j), i <= j < 12, row-major over the
-// upper triangle.
-constexpr int G156 = 156;
-
-__host__ __device__ constexpr int upper12(int i, int j) { return 12 * i - i * (i - 1) / 2 + (j - i); }
-
-// Fused update: as k_lobpcg_update4 (four threads per row, thread j writes
-// column j), and thread j accumulates the products whose first factor is
-// column j of X, R or P: 24 slots of S (u <= v blocks of [X R P], all four
-// columns b of block v, b >= j when u == v) and 16 of G (AX columns b >= j
-// against X; AP against X and R, and AP columns b >= j against P).  The row's
-// other columns come from its three partner lanes by shuffles.
-constexpr int FU_SLOTS = 40;
-
-template <class XT>
-__global__ void __launch_bounds__(256) k_lobpcg_update4g(LobpcgBlocks<XT> b, const LobpcgCtrl* __restrict__ ctrl,
-                                                         int64_t n, int init_mode, double* __restrict__ partial) {
-  __shared__ double sC[3][4][4];
-  __shared__ double sLam[4];
-  __shared__ int sF[4];
-  __shared__ double red[8][4][FU_SLOTS];
-  for (int t = threadIdx.x; t < G156; t += blockDim.x) partial[static_cast<int64_t>(blockIdx.x) * G156 + t] = 0.0;
-  if (threadIdx.x == 0) {
-    sF[0] = ctrl->done;
-    sF[1] = ctrl->copy_best;
-    sF[2] = ctrl->has_p;
-    sF[3] = ctrl->m;
-  }
-  if (threadIdx.x < 48) {
-    const int w = threadIdx.x / 16, r = (threadIdx.x / 4) % 4, c = threadIdx.x % 4;
-    const double* src = w == 0 ? ctrl->Cx : (w == 1 ? ctrl->Cr : ctrl->Cp);
-    sC[w][r][c] = src[r * MAXM + c];
-  }
-  if (threadIdx.x < 4) sLam[threadIdx.x] = ctrl->lam[threadIdx.x];
-  __syncthreads();
-  const int done = sF[0], copy_best = sF[1], use_p = sF[2], m = sF[3];
-  if (done && !copy_best) return;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int j = lane & 3;
-  const int base = lane & ~3;
-  double acc[FU_SLOTS];
-#pragma unroll
-  for (int q = 0; q < FU_SLOTS; ++q) acc[q] = 0.0;
-  const int64_t total = n * 4;
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;  // multiple of 32
-  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; (t & ~int64_t(31)) < total;
-       t += stride) {
-    const bool valid = t < total;
-    const int64_t i = valid ? (t >> 2) : 0;
-    const int64_t o = i * 4;
-    if (valid && copy_best) b.Xbest[o + j] = b.X[o + j];
-    if (done) continue;  // uniform
-    double x[4], ax[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      x[c] = static_cast<double>(b.X[o + c]);
-      ax[c] = static_cast<double>(b.AX[o + c]);
-    }
-    double pn = 0.0, apn = 0.0;
-    if (!init_mode) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        pn = fma(static_cast<double>(b.R[o + c]), sC[1][c][j], pn);
-        apn = fma(static_cast<double>(b.AR[o + c]), sC[1][c][j], apn);
-      }
-      if (use_p) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          pn = fma(static_cast<double>(b.P[o + c]), sC[2][c][j], pn);
-          apn = fma(static_cast<double>(b.AP[o + c]), sC[2][c][j], apn);
-        }
-      }
-    }
-    double xn = pn, axn = apn;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      xn = fma(x[c], sC[0][c][j], xn);
-      axn = fma(ax[c], sC[0][c][j], axn);
-    }
-    __syncwarp();
-    const bool active = j < m;
-    const XT xs = static_cast<XT>(active ? xn : 0.0);
-    const XT axs = static_cast<XT>(active ? axn : 0.0);
-    const XT rs = static_cast<XT>(active ? static_cast<double>(axs) - sLam[j] * static_cast<double>(xs) : 0.0);
-    // the values the next Gram reads: as stored (P and AP stay zero in init mode)
-    double v[5];
-    v[0] = static_cast<double>(xs);
-    v[1] = static_cast<double>(rs);
-    v[2] = 0.0;
-    v[3] = static_cast<double>(axs);
-    v[4] = 0.0;
-    if (valid) {
-      b.X[o + j] = xs;
-      b.AX[o + j] = axs;
-      b.R[o + j] = rs;
-      if (!init_mode) {
-        const XT ps = static_cast<XT>(active ? pn : 0.0);
-        const XT aps = static_cast<XT>(active ? apn : 0.0);
-        b.P[o + j] = ps;
-        b.AP[o + j] = aps;
-        v[2] = static_cast<double>(ps);
-        v[4] = static_cast<double>(aps);
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < 5; ++q) v[q] = 0.0;
-    }
-    // the row's four columns of X, R, P, AX, AP in every lane of the row
-    double row[5][4];
-#pragma unroll
-    for (int q = 0; q < 5; ++q)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) row[q][c] = __shfl_sync(0xffffffffu, v[q], base + c);
-    int slot = 0;
-#pragma unroll
-    for (int u = 0; u < 3; ++u)
-#pragma unroll
-      for (int vb = u; vb < 3; ++vb)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (vb > u || c >= j) acc[slot] = fma(v[u], row[vb][c], acc[slot]);
-          ++slot;
-        }
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {  // X^T AX, b >= j
-      if (c >= j) acc[slot] = fma(v[0], row[3][c], acc[slot]);
-      ++slot;
-    }
-#pragma unroll
-    for (int u = 0; u < 3; ++u)  // [X R P]^T AP (b >= j for P)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        if (u < 2 || c >= j) acc[slot] = fma(v[u], row[4][c], acc[slot]);
-        ++slot;
-      }
-  }
-  if (done) return;  // uniform: the partial row stays zero
-  // lanes of the same column j: sum over the warp, then over warps in order
-#pragma unroll
-  for (int q = 0; q < FU_SLOTS; ++q) {
-    double a = acc[q];
-    a += __shfl_xor_sync(0xffffffffu, a, 4);
-    a += __shfl_xor_sync(0xffffffffu, a, 8);
-    a += __shfl_xor_sync(0xffffffffu, a, 16);
-    if (lane < 4) red[warp][lane][q] = a;
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < 4 * FU_SLOTS; t += blockDim.x) {
-    const int a = t / FU_SLOTS, q = t % FU_SLOTS;
-    // slot q of column a -> entry
-    int e = -1;
-    if (q < 24) {
-      const int pair = q / 4, c = q % 4;  // (u, v) pairs in order (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
-      const int u = pair < 3 ? 0 : (pair < 5 ? 1 : 2);
-      const int vb = pair < 3 ? pair : (pair < 5 ? pair - 2 : 2);
-      if (vb > u || c >= a) e = upper12(u * 4 + a, vb * 4 + c);
-    } else if (q < 28) {
-      const int c = q - 24;
-      if (c >= a) e = 78 + upper12(a, c);
-    } else {
-      const int u = (q - 28) / 4, c = (q - 28) % 4;
-      if (u < 2 || c >= a) e = 78 + upper12(u * 4 + a, 8 + c);
-    }
-    if (e < 0) continue;
-    double s = 0.0;
-    for (int w = 0; w < 8; ++w) s += red[w][a][q];
-    partial[static_cast<int64_t>(blockIdx.x) * G156 + e] = s;
-  }
-}
-
-// The Gram entries that need AR: X^T AR (16) and the upper triangle of
-// R^T AR (10), one row per thread, CTA partial rows in the 156-entry layout.
-constexpr int AR_SLOTS = 26;
-constexpr int AR_THREADS = 256;
-
-template <class XT>
-__device__ __forceinline__ void load4(const XT* p, double (&v)[4]) {
-  if constexpr (sizeof(XT) == 8) {
-    const double4 t = *reinterpret_cast<const double4*>(p);
-    v[0] = t.x;
-    v[1] = t.y;
-    v[2] = t.z;
-    v[3] = t.w;
-  } else {
-    const float4 t = *reinterpret_cast<const float4*>(p);
-    v[0] = t.x;
-    v[1] = t.y;
-    v[2] = t.z;
-    v[3] = t.w;
-  }
-}
-
-template <class XT>
-__global__ void __launch_bounds__(AR_THREADS) k_gram_ar4(const XT* __restrict__ X, const XT* __restrict__ R,
-                                                         const XT* __restrict__ AR, int64_t n,
-                                                         double* __restrict__ partial, const int* __restrict__ stop) {
-  if (stop != nullptr && *stop != 0) return;
-  __shared__ double red[AR_THREADS / 32][AR_SLOTS];
-  double acc[AR_SLOTS];
-#pragma unroll
-  for (int q = 0; q < AR_SLOTS; ++q) acc[q] = 0.0;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * AR_THREADS + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * AR_THREADS) {
-    double x[4], r[4], ar[4];
-    load4(X + i * 4, x);
-    load4(R + i * 4, r);
-    load4(AR + i * 4, ar);
-    int q = 0;
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        acc[q] = fma(x[a], ar[c], acc[q]);
-        ++q;
-      }
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int c = a; c < 4; ++c) {
-        acc[q] = fma(r[a], ar[c], acc[q]);
-        ++q;
-      }
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < AR_SLOTS; ++q) {
-    const double s = warp_sum(acc[q]);
-    if (lane == 0) red[warp][q] = s;
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < G156; t += AR_THREADS) {
-    // entry t: one of the 26 slots, or zero
-    int q = -1;
-    if (t >= 78) {
-      const int e = t - 78;
-      for (int a = 0; a < 4 && q < 0; ++a)
-        for (int c = 0; c < 4; ++c)
-          if (upper12(a, 4 + c) == e) q = a * 4 + c;
-      int k = 16;
-      for (int a = 0; a < 4 && q < 0; ++a)
-        for (int c = a; c < 4; ++c, ++k)
-          if (upper12(4 + a, 4 + c) == e) q = k;
-    }
-    double s = 0.0;
-    if (q >= 0)
-      for (int w = 0; w < AR_THREADS / 32; ++w) s += red[w][q];
-    partial[static_cast<int64_t>(blockIdx.x) * G156 + t] = s;
-  }
-}
-
-// Adds the partial rows of the fused update (nu CTAs) and of k_gram_ar4 (na
-// CTAs) in CTA order and writes S and G (12 x 12 each, mirrored).  A CTA
-// takes 32 entries: warp w adds CTAs w, w + 8, ..., then the warp sums are
-// added in warp order.
-__global__ void __launch_bounds__(256) k_gram156_reduce(const double* __restrict__ pu, int nu,
-                                                        const double* __restrict__ pa, int na,
-                                                        double* __restrict__ out, const int* __restrict__ stop) {
-  if (stop != nullptr && *stop != 0) return;
-  __shared__ double red[8][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int e = blockIdx.x * 32 + lane;
-  double s = 0.0;
-  if (e < G156) {
-    for (int c = warp; c < nu; c += 8) s += pu[static_cast<int64_t>(c) * G156 + e];
-    for (int c = warp; c < na; c += 8) s += pa[static_cast<int64_t>(c) * G156 + e];
-  }
-  red[warp][lane] = s;
-  __syncthreads();
-  if (warp != 0 || e >= G156) return;
-  double v = 0.0;
-#pragma unroll
-  for (int w = 0; w < 8; ++w) v += red[w][lane];
-  const int h = e < 78 ? 0 : 1;
-  int rem = e - 78 * h, i = 0;
-  while (rem >= 12 - i) {
-    rem -= 12 - i;
-    ++i;
-  }
-  const int j = i + rem;
-  double* o = out + h * 144;
-  o[i * 12 + j] = v;
-  o[j * 12 + i] = v;
-}
-
 template <class XT>
 __global__ void k_combine(const XT* in0, const XT* in1, const XT* in2, const double* c0, const double* c1,
                           const double* c2, int nin, XT* out, int m_in, int m_out, int cstride, int ld,
@@ -1853,68 +1559,6 @@ void lobpcg_update_dev(const Exec& ex, const LobpcgBlocks<XT>& b, const LobpcgCt
 }
 
 // explicit instantiations
-bool fused_gram_enabled() {
-  const char* e = std::getenv("SPECTRAL_INIT_GRAM");
-  if (e == nullptr) return true;
-  const std::string v(e);
-  return v != "task" && v != "tile";
-}
-
-template <class XT>
-int update4g_grid(const Exec& ex) {
-  static std::atomic<int> resident[2][64];
-  const int ti = sizeof(XT) == 8 ? 1 : 0;
-  SI_REQUIRE(ex.device >= 0 && ex.device < 64, SI_INVALID_ARGUMENT, "update: device ordinal");
-  if (resident[ti][ex.device] == 0) {
-    int r = 0;
-    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_lobpcg_update4g<XT>, 256, 0));
-    resident[ti][ex.device] = std::max(1, r);
-  }
-  return ex.sms * resident[ti][ex.device].load();
-}
-
-template <class XT>
-int gram_ar4_grid(const Exec& ex) {
-  static std::atomic<int> resident[2][64];
-  const int ti = sizeof(XT) == 8 ? 1 : 0;
-  SI_REQUIRE(ex.device >= 0 && ex.device < 64, SI_INVALID_ARGUMENT, "gram: device ordinal");
-  if (resident[ti][ex.device] == 0) {
-    int r = 0;
-    SI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gram_ar4<XT>, AR_THREADS, 0));
-    resident[ti][ex.device] = std::max(1, r);
-  }
-  return ex.sms * resident[ti][ex.device].load();
-}
-
-template <class XT>
-void lobpcg_update4g_dev(const Exec& ex, const LobpcgBlocks<XT>& b, const LobpcgCtrl* ctrl, int64_t n, int init_mode,
-                         double* pu, int nu) {
-  if (n == 0) return;
-  k_lobpcg_update4g<XT><<<nu, 256, 0, ex.stream>>>(b, ctrl, n, init_mode, pu);
-  SI_LAUNCH_CHECK();
-}
-
-template <class XT>
-void gram_ar4_dev(const Exec& ex, const XT* X, const XT* R, const XT* AR, int64_t n, double* pa, int na,
-                  const double* pu, int nu, double* out, const int* stop) {
-  k_gram_ar4<XT><<<na, AR_THREADS, 0, ex.stream>>>(X, R, AR, n, pa, stop);
-  SI_LAUNCH_CHECK();
-  k_gram156_reduce<<<(G156 + 31) / 32, 256, 0, ex.stream>>>(pu, nu, pa, na, out, stop);
-  SI_LAUNCH_CHECK();
-}
-
-template int update4g_grid<double>(const Exec&);
-template int update4g_grid<float>(const Exec&);
-template int gram_ar4_grid<double>(const Exec&);
-template int gram_ar4_grid<float>(const Exec&);
-template void lobpcg_update4g_dev<double>(const Exec&, const LobpcgBlocks<double>&, const LobpcgCtrl*, int64_t, int,
-                                          double*, int);
-template void lobpcg_update4g_dev<float>(const Exec&, const LobpcgBlocks<float>&, const LobpcgCtrl*, int64_t, int,
-                                         double*, int);
-template void gram_ar4_dev<double>(const Exec&, const double*, const double*, const double*, int64_t, double*, int,
-                                   const double*, int, double*, const int*);
-template void gram_ar4_dev<float>(const Exec&, const float*, const float*, const float*, int64_t, double*, int,
-                                  const double*, int, double*, const int*);
 template void gram_dev<double>(const Exec&, GramWork&, GramMode, const double* const*, int, int, int, int, int64_t,
                                double*, const int*);
 template void gram_dev<float>(const Exec&, GramWork&, GramMode, const float* const*, int, int, int, int, int64_t,

@@ -248,22 +248,6 @@ struct LobpcgBlocks {
 template <class XT>
 void lobpcg_update_dev(const Exec& ex, const LobpcgBlocks<XT>& b, const LobpcgCtrl* ctrl, int ld, int64_t n,
                        int init_mode);
-// 4-column blocks with the Gram folded into the update (default;
-// SPECTRAL_INIT_GRAM=task / tile run the separate Gram kernels instead): the
-// update also writes one 156-entry partial row per CTA (nu CTAs, from
-// update4g_grid) of the next iteration's Gram; gram_ar4_dev adds the entries
-// that need AR (na CTAs, from gram_ar4_grid) and writes S and G (12 x 12).
-bool fused_gram_enabled();
-template <class XT>
-int update4g_grid(const Exec& ex);
-template <class XT>
-int gram_ar4_grid(const Exec& ex);
-template <class XT>
-void lobpcg_update4g_dev(const Exec& ex, const LobpcgBlocks<XT>& b, const LobpcgCtrl* ctrl, int64_t n, int init_mode,
-                         double* pu, int nu);
-template <class XT>
-void gram_ar4_dev(const Exec& ex, const XT* X, const XT* R, const XT* AR, int64_t n, double* pa, int na,
-                  const double* pu, int nu, double* out, const int* stop);
 
 // ---- cg.cu -----------------------------------------------------------------------
 // Block CG on M Y = B (M symmetric positive definite, the operator with its

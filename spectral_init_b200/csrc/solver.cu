@@ -65,11 +65,6 @@ struct LobpcgState {
   DevBuf<double> gram;
   DevBuf<LobpcgCtrl> ctrl, aux;
   GramWork gw;
-  // Gram folded into the update (4-column blocks): partial rows of the update
-  // (fnu CTAs) and of the AR products (fna CTAs)
-  DevBuf<double> fpu, fpa;
-  int fnu = 0, fna = 0;
-  bool fused = false;
   void alloc(const Exec& ex, int64_t n_, int m_, int ld_) {
     n = n_;
     m = m_;
@@ -85,13 +80,6 @@ struct LobpcgState {
     gram.alloc(2 * (3 * MAXM) * (3 * MAXM), ex.stream);
     ctrl.alloc(1, ex.stream);
     aux.alloc(1, ex.stream);
-    fused = ld == 4 && m == 4 && fused_gram_enabled();
-    if (fused) {
-      fnu = update4g_grid<XT>(ex);
-      fna = gram_ar4_grid<XT>(ex);
-      fpu.alloc(static_cast<size_t>(fnu) * 156, ex.stream);
-      fpa.alloc(static_cast<size_t>(fna) * 156, ex.stream);
-    }
   }
   const int* stop() const { return &ctrl.get()->done; }
   LobpcgBlocks<XT> blocks() {
@@ -154,21 +142,15 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
     gram_dev<XT>(ex, s.gw, GRAM_SYM2, blk, 1, 2, s.m, s.ld, s.n, s.gram.get());
   }
   small_step_dev(ex, s.ctrl.get(), s.gram.get(), 1, SM_INIT, s.m);
-  if (s.fused) lobpcg_update4g_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.n, 1, s.fpu.get(), s.fnu);
-  else lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 1);
+  lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 1);
   const XT* blk6[6] = {s.X.get(), s.R.get(), s.P.get(), s.AX.get(), s.AR.get(), s.AP.get()};
   auto enqueue_iterations = [&](int count) {
     for (int b = 0; b < count; ++b) {
       if (apply != nullptr) (*apply)(s.R.get(), s.AR.get());
       else spmm_dev<XT>(ex, A, s.R.get(), s.AR.get(), s.ld, s.m, ep, s.stop(), f32vals);
-      if (s.fused)
-        gram_ar4_dev<XT>(ex, s.X.get(), s.R.get(), s.AR.get(), s.n, s.fpa.get(), s.fna, s.fpu.get(), s.fnu,
-                         s.gram.get(), s.stop());
-      else
-        gram_dev<XT>(ex, s.gw, GRAM_SYM2, blk6, 3, 6, s.m, s.ld, s.n, s.gram.get(), s.stop());
+      gram_dev<XT>(ex, s.gw, GRAM_SYM2, blk6, 3, 6, s.m, s.ld, s.n, s.gram.get(), s.stop());
       small_step_dev(ex, s.ctrl.get(), s.gram.get(), 3, SM_ITER, s.m);
-      if (s.fused) lobpcg_update4g_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.n, 0, s.fpu.get(), s.fnu);
-      else lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 0);
+      lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 0);
     }
   };
   // One iteration's first pass allocates every work buffer; later batches are

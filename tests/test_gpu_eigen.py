@@ -287,20 +287,17 @@ def test_lobpcg_wide_blocks(gpu_ctx, nc, block, precision):
         assert resid(lap, vecs[:, j], vals[j]) < 1e-5
 
 
-@pytest.mark.parametrize("variant", ["fused", "task", "tile"])
+@pytest.mark.parametrize("variant", ["task", "tile"])
 @pytest.mark.parametrize("small", ["warp", "cta", "reg"])
 def test_lobpcg_kernel_variants_agree(gpu_ctx, monkeypatch, variant, small):
-    """The 4-column LOBPCG iteration with each Gram path (folded into the
-    update with the AR products after the SpMM, default; the task-split Gram
-    kernel, SPECTRAL_INIT_GRAM=task; the register-tiled one, =tile) and each
-    small step (one warp with the Gram in shared memory,
-    SPECTRAL_INIT_SMALL_STEP=warp; one 128-thread CTA, the default; one warp
-    in registers, =reg) converges to the dense eigenpairs."""
+    """The 4-column LOBPCG iteration with either Gram kernel (task-split warps,
+    default; register-tiled, SPECTRAL_INIT_GRAM=tile) and each small step (one
+    warp with the Gram in shared memory, SPECTRAL_INIT_SMALL_STEP=warp; one
+    128-thread CTA, the default; one warp in registers, =reg) converges to the
+    dense eigenpairs."""
     import spectral_init_b200 as si
-    if variant == "fused":
-        monkeypatch.delenv("SPECTRAL_INIT_GRAM", raising=False)
-    else:
-        monkeypatch.setenv("SPECTRAL_INIT_GRAM", variant)
+    if variant == "tile":
+        monkeypatch.setenv("SPECTRAL_INIT_GRAM", "tile")
     monkeypatch.setenv("SPECTRAL_INIT_SMALL_STEP", small)
     lap = load_csr("blobs_connected_2000", "comp_b_laplacian.npz")
     cfg = si.SpectralInitConfig(force_level=1, tol=1e-10)
