@@ -197,17 +197,42 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
       if (e) cudaGraphExecDestroy(e);
     }
   } guard{exec};
+  // One replay stays queued ahead of the host's look at the stop flag: the
+  // flag after replay k is read while replay k + 1 runs, so the device never
+  // waits for the host between batches (a replay queued after convergence
+  // finds the flag set and its kernels return at once).  The flags land in a
+  // small pinned buffer of the calling thread, kept for the process.
+  static thread_local int* flags = nullptr;
+  if (flags == nullptr)
+    SI_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&flags), 2 * sizeof(int), cudaHostAllocDefault));
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  struct EventGuard {
+    cudaEvent_t* e;
+    ~EventGuard() {
+      for (int i = 0; i < 2; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } eguard{ev};
+  SI_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  SI_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
   int launched = 1;
-  for (;;) {
-    int done = 0;
-    SI_CUDA(cudaMemcpyAsync(&done, s.stop(), sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
-    SI_CUDA(cudaStreamSynchronize(ex.stream));
-    if (done) break;
-    SI_REQUIRE(launched <= maxiter + 2 * kGraphBatch, SI_CUDA_ERROR, "lobpcg: device loop did not terminate");
+  auto replay = [&](int slot) {
+    SI_REQUIRE(launched <= maxiter + 3 * kGraphBatch, SI_CUDA_ERROR, "lobpcg: device loop did not terminate");
     SI_CUDA(cudaGraphLaunch(exec, ex.stream));
     g_kernel_launches.fetch_add(per_replay);
     tl_kernel_launches += per_replay;
     launched += kGraphBatch;
+    SI_CUDA(cudaMemcpyAsync(&flags[slot], s.stop(), sizeof(int), cudaMemcpyDeviceToHost, ex.stream));
+    SI_CUDA(cudaEventRecord(ev[slot], ex.stream));
+  };
+  int slot = 0;
+  replay(0);
+  replay(1);
+  for (;;) {
+    SI_CUDA(cudaEventSynchronize(ev[slot]));
+    if (flags[slot]) break;
+    replay(slot);
+    slot ^= 1;
   }
   return finish_core(ex, s, spmm_calls);
 }
