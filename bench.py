@@ -883,6 +883,7 @@ def run_learned_eval(a):
             cfg.warm_start = warm
             cfg.tol = a.tol
             cfg.learned_filter = a.learned_filter
+            cfg.mixed_switch_tol = a.switch_tol
             k = a.nc + 1
             vals = (C.c_double * k)()
             vecs = torch.empty(a.n, k, dtype=torch.float64, device=dev)
