@@ -214,7 +214,7 @@ struct LobpcgCtrl {
   int iter, done, status, has_p;
   int copy_best, mode, best_iter, n_active;
   int p_valid;  // P holds a search direction from a previous update
-  int stall_window;  // > 0: stop when the best residual sum is this many iterations old
+  int pad_;
   int active[MAXM];
   double lam[MAXM];
   double rnorm[MAXM];

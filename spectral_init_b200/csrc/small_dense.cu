@@ -920,9 +920,6 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
     } else if (ctrl->iter >= ctrl->maxiter) {
       done = 1;
       ctrl->status = ST_MAXITER;
-    } else if (ctrl->stall_window > 0 && ctrl->best_iter >= 0 && ctrl->iter - ctrl->best_iter >= ctrl->stall_window) {
-      done = 1;  // no better iterate for stall_window iterations (the f32 phase near its floor)
-      ctrl->status = ST_MAXITER;
     }
     ctrl->done = done;
     sdone = done;

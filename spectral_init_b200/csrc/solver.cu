@@ -47,8 +47,6 @@ namespace {
 
 int pick_ld(int m) { return m <= 4 ? 4 : (m <= 8 ? 8 : 16); }
 
-constexpr int F32_STALL_WINDOW = 30;
-
 // Block width: the wanted k vectors plus guard vectors up to the padded row
 // width when the problem is large enough (guards raise the convergence rate
 // of the wanted pairs at no extra memory traffic: rows are padded anyway).
@@ -120,7 +118,7 @@ CoreOutcome finish_core(const Exec& ex, LobpcgState<XT>& s, int& spmm_calls) {
 template <class XT>
 CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int k_wanted, double tol, int maxiter,
                         bool largest, double chol_tol, bool f32vals, int& spmm_calls,
-                        const std::function<void(const XT*, XT*)>* apply = nullptr, int stall_window = 0) {
+                        const std::function<void(const XT*, XT*)>* apply = nullptr) {
   LobpcgCtrl h;
   std::memset(&h, 0, sizeof(h));
   h.m = s.m;
@@ -129,7 +127,6 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
   h.largest = largest ? 1 : 0;
   h.tol = tol;
   h.chol_tol = chol_tol;
-  h.stall_window = stall_window;
   h.best_sum = DBL_MAX;
   SI_CUDA(cudaMemcpyAsync(s.ctrl.get(), &h, sizeof(h), cudaMemcpyHostToDevice, ex.stream));
   s.P.zero();
@@ -414,11 +411,7 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
     const double switch_tol = cfg.mixed_switch_tol > 0.0 ? cfg.mixed_switch_tol : (learned ? 1e-5 : 1e-4);
     const int maxiter32 = static_cast<int>(std::min<int64_t>(5 * n, cfg.max_iterations > 0 ? cfg.max_iterations
                                                                                            : LOBPCG_RESTART_MAXITER_CAP));
-    // the f32 phase also ends when its best iterate is F32_STALL_WINDOW
-    // iterations old: near the f32 floor the residual stops falling, and the
-    // f64 phase continues from the best iterate
-    CoreOutcome o32 = lobpcg_core<float>(ex, A, s32, k, switch_tol, maxiter32, false, 1e-10, true, st.spmm_calls,
-                                         nullptr, F32_STALL_WINDOW);
+    CoreOutcome o32 = lobpcg_core<float>(ex, A, s32, k, switch_tol, maxiter32, false, 1e-10, true, st.spmm_calls);
     st.fp32_iterations += o32.iterations;
     st.iterations += o32.iterations;
     if (o32.best_valid) {
