@@ -118,7 +118,7 @@ CoreOutcome finish_core(const Exec& ex, LobpcgState<XT>& s, int& spmm_calls) {
 template <class XT>
 CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int k_wanted, double tol, int maxiter,
                         bool largest, double chol_tol, bool f32vals, int& spmm_calls,
-                        const std::function<void(const XT*, XT*)>* apply = nullptr, const XT* carry_p = nullptr) {
+                        const std::function<void(const XT*, XT*)>* apply = nullptr) {
   LobpcgCtrl h;
   std::memset(&h, 0, sizeof(h));
   h.m = s.m;
@@ -143,16 +143,6 @@ CoreOutcome lobpcg_core(const Exec& ex, const OpDev& A, LobpcgState<XT>& s, int 
   }
   small_step_dev(ex, s.ctrl.get(), s.gram.get(), 1, SM_INIT, s.m);
   lobpcg_update_dev<XT>(ex, s.blocks(), s.ctrl.get(), s.ld, s.n, 1);
-  if (carry_p != nullptr && apply == nullptr) {
-    // continue with the search direction of the pass this one takes over from
-    // (the f32 phase of a mixed solve): P as given, AP recomputed, so the
-    // first iteration's Rayleigh-Ritz already spans [X R P]
-    SI_CUDA(cudaMemcpyAsync(s.P.get(), carry_p, sizeof(XT) * s.n * s.ld, cudaMemcpyDeviceToDevice, ex.stream));
-    spmm_dev<XT>(ex, A, s.P.get(), s.AP.get(), s.ld, s.m, ep, nullptr, f32vals);
-    ++spmm_calls;
-    const int one = 1;
-    SI_CUDA(cudaMemcpyAsync(&s.ctrl.get()->p_valid, &one, sizeof(int), cudaMemcpyHostToDevice, ex.stream));
-  }
   const XT* blk6[6] = {s.X.get(), s.R.get(), s.P.get(), s.AX.get(), s.AR.get(), s.AP.get()};
   auto enqueue_iterations = [&](int count) {
     for (int b = 0; b < count; ++b) {
@@ -404,7 +394,6 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
   std::vector<int> all_cols(m);
   std::iota(all_cols.begin(), all_cols.end(), 0);
 
-  DevBuf<double> p_carry;  // the f32 phase's search direction, handed to the first f64 pass
   if (mixed) {
     // f32 bulk: Chebyshev filter and LOBPCG on f32 blocks and f32 matrix
     // values (f64 accumulation, f64 Gram and small steps), then the f64
@@ -430,10 +419,6 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
     } else {
       gather_columns_dev<float, double>(ex, s32.X.get(), ld, s.X.get(), ld, n, all_cols);
     }
-    if (o32.iterations > 0) {
-      p_carry.alloc(static_cast<size_t>(n) * ld, ex.stream);
-      gather_columns_dev<float, double>(ex, s32.P.get(), ld, p_carry.get(), ld, n, all_cols);
-    }
   } else if (n >= CHEB_MIN_N && (!learned || cfg.learned_chebyshev)) {
     chebyshev_start<double>(ex, A, s, false, st.spmm_calls);
   }
@@ -455,9 +440,7 @@ bool lobpcg_solve_dev(const Exec& ex, const OpDev& op_in, int n_components, uint
       }
     }
     const int maxiter = static_cast<int>(std::min<int64_t>(5 * n, cap));
-    const double* carry = (restart == 0 && p_carry.get() != nullptr) ? p_carry.get() : nullptr;
-    CoreOutcome o = lobpcg_core<double>(ex, A, s, k, tol32, maxiter, false, 1e-14, false, st.spmm_calls, nullptr,
-                                        carry);
+    CoreOutcome o = lobpcg_core<double>(ex, A, s, k, tol32, maxiter, false, 1e-14, false, st.spmm_calls);
     st.iterations += o.iterations;
     if (!o.best_valid) break;  // breakdown before any iterate: the crate's Err((_, None))
     bool accept = o.status == ST_CONVERGED;
