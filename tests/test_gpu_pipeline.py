@@ -155,3 +155,37 @@ def test_deterministic_for_a_seed(gpu_ctx):
     a = si.spectral_init(g, 2, 7, ctx=gpu_ctx)
     b = si.spectral_init(g, 2, 7, ctx=gpu_ctx)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_many_uneven_components_every_residual(gpu_ctx, precision):
+    """The batched multi-component workload at reduced scale: 60 disconnected
+    fuzzy-kNN components with sizes log-uniform in [20, 20 000] (each a
+    Gaussian mixture of 1-10 clusters in 20-D), full pipeline with the spectral
+    meta-embedding, plain FP64 and mixed precision.  Every component's
+    eigensolve passes the crate's residual gate (the report carries the worst
+    component's residual and the highest level used), every component is
+    found, and the embedding is finite."""
+    import ctypes as C
+    import torch
+    from spectral_init_b200 import synthetic
+    from spectral_init_b200._lib import SiConfig, SiCsrF32, SiReport
+    dev = torch.device("cuda", gpu_ctx.device)
+    ip, ix, dv, n, pts, sizes = synthetic.multi_component_graph_gpu(60, 20, 20_000, 20, 15, 7, device=dev)
+    g = SiCsrF32(n, int(ix.numel()), ip.data_ptr(), ix.data_ptr(), dv.data_ptr())
+    out = torch.empty(n, 2, dtype=torch.float32, device=dev)
+    cfg = SiConfig()
+    gpu_ctx.lib.si_config_default(C.byref(cfg))
+    cfg.precision = precision
+    rep = SiReport()
+    torch.cuda.synchronize()
+    gpu_ctx.check(gpu_ctx.lib.si_spectral_init_device(gpu_ctx.ptr, C.byref(g), 2, 42, pts.data_ptr(), pts.shape[1],
+                                                      C.byref(cfg), out.data_ptr(), C.byref(rep)))
+    gpu_ctx.synchronize()
+    assert rep.n_components_graph == 60
+    assert rep.max_residual <= 1e-5, rep.max_residual
+    assert 0 <= rep.level <= 1
+    emb = out.cpu().numpy()
+    assert np.all(np.isfinite(emb))
+    assert np.abs(emb).max() <= 10.0 + 1e-3 * 10.0
