@@ -7,14 +7,21 @@ n_components = 2 (the crate's default embedding), seed 42.
 
 One step = one eigensolve (solve_eigenproblem: Chebyshev-filtered start,
 block LOBPCG, Rayleigh-Ritz refinement, FP64 residual gate <= 1e-5) with the
-Laplacian already resident in HBM.  `value` is the mean device time of the
-mixed-precision solve (f32 bulk + f64 refinement); the plain FP64 solve, the
-SpMM bandwidth (the roofline kernel), the end-to-end C-ABI call with host
-buffers, and the CPU baseline (the restated reference path on the host cores)
-are reported beside it.
+Laplacian already resident in HBM; step i solves with seed --seed + i, the
+same seeds in every leg (the iteration count moves by tens of percent with
+the random start).  `value` is the mean device time of the learned-start
+mixed-precision solve (f32 bulk + f64 refinement) at --tol (1e-7, where the
+subspace meets 1e-4 against the certified oracle); the plain FP64 solve at the
+crate's 1e-5 and at --tol, the random-start mixed solve, the SpMM bandwidth
+(the roofline kernel), the end-to-end C-ABI call with host buffers, and the
+CPU baseline (the restated reference path on the host cores) are reported
+beside it.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
     python bench.py --spmm-profile      # small SpMM-only run for ncu captures
+    python bench.py --profile-solve [--solve-seed S --profile-repeat R --block-size B --switch-tol T]
+    python bench.py --configs | --components | --dense | --learned-eval G | --accuracy-sweep
+    python bench.py --cpu-only --cpu-threads T   # the CPU baseline alone
 """
 from __future__ import annotations
 
