@@ -249,15 +249,16 @@ def test_spmm_sliced_variants(gpu_ctx, kernel, matrix, width, prec):
 
 def test_spmm_tuning_file(gpu_ctx, monkeypatch, tmp_path):
     """SPECTRAL_INIT_SPMM_TUNE_FILE: the autotuner appends the choice it timed,
-    keyed by the operator's shape (n, nnz, width, value and block types)."""
+    keyed by the operator's shape (n, nnz, width, value and block types);
+    operators of at least 2^22 stored entries are timed."""
     import torch
     import spectral_init_b200 as si
     path = tmp_path / "tune.txt"
     monkeypatch.setenv("SPECTRAL_INIT_SPMM_TUNE_FILE", str(path))
     monkeypatch.delenv("SPECTRAL_INIT_SPMM_KERNEL", raising=False)
     rng = np.random.default_rng(21)
-    n = 25_013  # a shape no other test uses
-    a = sp.random(n, n, density=12.0 / n, random_state=rng, format="csr")
+    n = 262_147  # a shape no other test uses, with enough entries (~4.7 M) to be timed
+    a = sp.random(n, n, density=9.0 / n, random_state=rng, format="csr")
     a = (a + a.T).tocsr()
     a.sort_indices()
     op = si.CsrOperator(a, diag=1.0, ctx=gpu_ctx)
