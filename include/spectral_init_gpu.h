@@ -193,8 +193,12 @@ si_status si_spmm_f32(si_ctx* ctx, const si_operator* op, const float* x, float*
 /* A device operator prepared for repeated products (the crate's CsrOperator,
  * src/operator.rs:174-228, holds its matrix across LinearOperator::apply
  * calls): the row partitions of the tiled / gather / panel kernels are built
- * once, the panel kernel's x windows once per block width.  The operator's
- * arrays must stay allocated and unchanged while the plan lives. */
+ * once; the sliced copy of the operator (the default kernel for operators the
+ * autotuner times, about the size of the index and value arrays again) and the
+ * panel kernel's x windows on first use, outside stream capture.  The
+ * operator's arrays must stay allocated and unchanged while the plan lives,
+ * and calls on one plan from several host threads must be serialised by the
+ * caller (the first calls build that state). */
 typedef struct si_operator_plan si_operator_plan;
 si_status si_operator_plan_create(si_ctx* ctx, const si_operator* op, si_operator_plan** out);
 void si_operator_plan_destroy(si_operator_plan* plan);
