@@ -778,10 +778,134 @@ __device__ bool warp_rr_general(const double* gb, const double* ga, int P, const
   return true;
 }
 
-// Rayleigh-Ritz of the small step: the shared-memory CTA routines (on a
-// single-warp CTA their barriers are warp-cheap), or, with REG, the
-// register-resident warp version (SPECTRAL_INIT_SMALL_STEP=reg).
-template <int NT, bool REG>
+// The generalised Rayleigh-Ritz of cta_rr_general with its serial sections
+// made parallel: the D-scale factors one per thread; a right-looking
+// Cholesky with one barrier per pivot (every thread recomputes the pivot, the
+// trailing update reads the unscaled pivot column, and the column scaling is
+// one pass at the end); L^-1 formed once, one column per thread, so that
+// C = L^-1 A L^-T and the Ritz vectors D L^-T V_sel are parallel matrix
+// products instead of three one-thread-per-column triangular solves; the
+// selection order by ranks.  Same results as cta_rr_general up to rounding.
+__device__ bool cta_rr_general_par(const double* gb, const double* ga, int P, const int* idx, int s, int nsel,
+                                   int largest, double chol_tol, SmallSmem sm, double* dsc, double* theta_out,
+                                   double* red, int* order, int* sflag) {
+  __shared__ double lsq[3 * MAXM];  // sqrt of the pivots, then 1 / L_jj
+  const int ld = sm.ld;
+  const int nt = blockDim.x;
+  if (threadIdx.x == 0) *sflag = 0;
+  for (int t = threadIdx.x; t < s * s; t += nt) {
+    const int i = t / s, j = t % s;
+    sm.B[i * ld + j] = gb[idx[i] * P + idx[j]];
+    sm.A[i * ld + j] = ga[idx[i] * P + idx[j]];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < s; i += nt) {
+    const double d = sm.B[i * ld + i];
+    const bool ok = d > 0.0 && isfinite(d);
+    if (!ok) atomicExch(sflag, 1);
+    dsc[i] = ok ? 1.0 / sqrt(d) : 0.0;
+  }
+  __syncthreads();
+  if (*sflag) return false;
+  for (int t = threadIdx.x; t < s * s; t += nt) {
+    const int i = t / s, j = t % s;
+    const double f = dsc[i] * dsc[j];
+    sm.B[i * ld + j] *= f;
+    sm.A[i * ld + j] *= f;
+  }
+  __syncthreads();
+  // ---- Cholesky, one barrier per pivot ----
+  for (int j = 0; j < s; ++j) {
+    const double piv = sm.B[j * ld + j];
+    if (!(piv > chol_tol)) return false;  // the same value in every thread
+    const double inv2 = 1.0 / piv;        // (b_ij / l_jj)(b_kj / l_jj) = b_ij b_kj / b_jj
+    if (threadIdx.x == 0) lsq[j] = sqrt(piv);
+    const int w = s - j - 1;
+    for (int t = threadIdx.x; t < w * w; t += nt) {
+      const int i = j + 1 + t / w, k = j + 1 + t % w;
+      if (k <= i) sm.B[i * ld + k] -= sm.B[i * ld + j] * sm.B[k * ld + j] * inv2;
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < s * s; t += nt) {  // finish the columns: l_ij = b_ij / sqrt(b_jj)
+    const int i = t / s, j = t % s;
+    if (i > j) sm.B[i * ld + j] /= lsq[j];
+    else if (i == j) sm.B[i * ld + i] = lsq[i];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < s; i += nt) lsq[i] = 1.0 / lsq[i];
+  __syncthreads();
+  // ---- M = L^-1 (lower), one column per thread, into Z ----
+  for (int c = threadIdx.x; c < s; c += nt) {
+    for (int i = 0; i < c; ++i) sm.Z[i * ld + c] = 0.0;
+    sm.Z[c * ld + c] = lsq[c];
+    for (int i = c + 1; i < s; ++i) {
+      double v = 0.0;
+      for (int k = c; k < i; ++k) v = fma(sm.B[i * ld + k], sm.Z[k * ld + c], v);
+      sm.Z[i * ld + c] = -v * lsq[i];
+    }
+  }
+  __syncthreads();
+  // keep M in B (L is no longer needed)
+  for (int t = threadIdx.x; t < s * s; t += nt) {
+    const int i = t / s, j = t % s;
+    sm.B[i * ld + j] = sm.Z[i * ld + j];
+  }
+  __syncthreads();
+  // ---- C = M A M^T: Y = M A into T, then C = Y M^T into A ----
+  for (int t = threadIdx.x; t < s * s; t += nt) {
+    const int i = t / s, j = t % s;
+    double v = 0.0;
+    for (int k = 0; k <= i; ++k) v = fma(sm.B[i * ld + k], sm.A[k * ld + j], v);
+    sm.T[i * ld + j] = v;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < s * s; t += nt) {
+    const int i = t / s, j = t % s;
+    if (j < i) continue;  // upper triangle, mirrored below
+    double v = 0.0;
+    for (int k = 0; k <= j; ++k) v = fma(sm.T[i * ld + k], sm.B[j * ld + k], v);
+    double u = 0.0;  // the (j, i) entry, for the symmetrised average
+    for (int k = 0; k <= i; ++k) u = fma(sm.T[j * ld + k], sm.B[i * ld + k], u);
+    const double a = 0.5 * (v + u);
+    sm.A[i * ld + j] = a;
+    sm.A[j * ld + i] = a;
+  }
+  __syncthreads();
+  cta_identity(sm.V, s, ld);
+  __syncthreads();
+  cta_jacobi_db(sm.A, sm.V, sm.T, sm.Z, s, ld, red);
+  // ---- selection by ranks (ascending, or descending for `largest`; ties by index) ----
+  for (int i = threadIdx.x; i < s; i += nt) {
+    const double di = sm.A[i * ld + i];
+    int rank = 0;
+    for (int j = 0; j < s; ++j) {
+      const double dj = sm.A[j * ld + j];
+      // ascending and stable; for `largest` the reverse of that order
+      const bool before = largest ? (dj > di || (dj == di && j > i)) : (dj < di || (dj == di && j < i));
+      rank += before ? 1 : 0;
+    }
+    order[rank] = i;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nsel; q += nt) theta_out[q] = sm.A[order[q] * ld + order[q]];
+  // ---- Z = D M^T V_sel ----
+  for (int t = threadIdx.x; t < s * nsel; t += nt) {
+    const int i = t / nsel, q = t % nsel;
+    const int c = order[q];
+    double v = 0.0;
+    for (int k = i; k < s; ++k) v = fma(sm.B[k * ld + i], sm.V[k * ld + c], v);
+    sm.Z[i * ld + q] = v * dsc[i];
+  }
+  __syncthreads();
+  return true;
+}
+
+// Rayleigh-Ritz of the small step: the shared-memory CTA routines (PAR: the
+// parallel form, the default for the CTA kernels; on a single-warp CTA their
+// barriers are warp-cheap), or, with REG, the register-resident warp version
+// (SPECTRAL_INIT_SMALL_STEP=reg).
+template <int NT, bool REG, bool PAR>
 __device__ bool rr_general(const double* gb, const double* ga, int P, const int* idx, int s, int nsel, int largest,
                            double chol_tol, SmallSmem sm, double* dsc, double* theta_out, double* red, double* rc,
                            double* rs, int* ra, int* rb, int* order, int* sflag) {
@@ -789,12 +913,16 @@ __device__ bool rr_general(const double* gb, const double* ga, int P, const int*
     if (s <= WRR)
       return warp_rr_general(gb, ga, P, idx, s, nsel, largest, chol_tol, sm.Z, sm.ld, sm.T, theta_out);
   }
+  if constexpr (PAR) {
+    if (s <= 3 * MAXM)
+      return cta_rr_general_par(gb, ga, P, idx, s, nsel, largest, chol_tol, sm, dsc, theta_out, red, order, sflag);
+  }
   return cta_rr_general(gb, ga, P, idx, s, nsel, largest, chol_tol, sm, dsc, theta_out, red, rc, rs, ra, rb, order,
                         sflag);
 }
 
 // `ctrl` points to the CTA's shared-memory copy of the control block.
-template <int NT, bool REG>
+template <int NT, bool REG, bool PAR>
 __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns, int mode,
                                 double* smem) {
   __shared__ double red[ST_WIDE / 32];
@@ -818,7 +946,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
   if (mode == SM_INIT) {
     for (int i = threadIdx.x; i < m; i += blockDim.x) idx[i] = i;
     __syncthreads();
-    const bool ok = rr_general<NT, REG>(gb, ga, P, idx, m, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc,
+    const bool ok = rr_general<NT, REG, PAR>(gb, ga, P, idx, m, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc,
                                    rs, ra, rb, order, &sflag);
     if (threadIdx.x == 0) {
       ctrl->iter = 0;
@@ -943,12 +1071,12 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
         if (ctrl->active[c]) idx[m + na + q++] = 2 * m + c;
     }
     __syncthreads();
-    ok = rr_general<NT, REG>(gb, ga, P, idx, m + 2 * na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs,
+    ok = rr_general<NT, REG, PAR>(gb, ga, P, idx, m + 2 * na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs,
                         ra, rb, order, &sflag);
     if (!ok) withp = 0;
   }
   if (!ok) {
-    ok = rr_general<NT, REG>(gb, ga, P, idx, m + na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs, ra,
+    ok = rr_general<NT, REG, PAR>(gb, ga, P, idx, m + na, m, ctrl->largest, ctrl->chol_tol, sm, dsc, theta, red, rc, rs, ra,
                         rb, order, &sflag);
   }
   if (!ok) {
@@ -985,7 +1113,7 @@ __device__ void small_step_body(LobpcgCtrl* ctrl, const double* __restrict__ gra
 
 // The control block is staged in shared memory for the whole step (the step
 // is a long chain of small dependent updates) and written back at the end.
-template <int NT, bool REG = false>
+template <int NT, bool REG = false, bool PAR = false>
 __global__ void __launch_bounds__(NT, 1) k_small_step(LobpcgCtrl* ctrl, const double* __restrict__ gram, int ns,
                                                    int mode) {
   extern __shared__ double smem[];
@@ -996,7 +1124,7 @@ __global__ void __launch_bounds__(NT, 1) k_small_step(LobpcgCtrl* ctrl, const do
   const double* src = reinterpret_cast<const double*>(ctrl);
   for (int i = threadIdx.x; i < W; i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  small_step_body<NT, REG>(&sctrl, gram, ns, mode, smem);
+  small_step_body<NT, REG, PAR>(&sctrl, gram, ns, mode, smem);
   __syncthreads();
   double* back = reinterpret_cast<double*>(ctrl);
   for (int i = threadIdx.x; i < W; i += blockDim.x) back[i] = dst[i];
@@ -1053,7 +1181,7 @@ int small_step_variant() {
   const char* e = std::getenv("SPECTRAL_INIT_SMALL_STEP");
   if (e == nullptr) return 1;
   const std::string v(e);
-  return v == "warp" ? 0 : (v == "reg" ? 2 : 1);
+  return v == "warp" ? 0 : (v == "reg" ? 2 : (v == "serial" ? 3 : 1));
 }
 
 void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns, int mode, int m) {
@@ -1065,6 +1193,10 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
                                  static_cast<int>(smem)));
     SI_CUDA(cudaFuncSetAttribute(k_small_step<ST_WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
+    SI_CUDA(cudaFuncSetAttribute(k_small_step<ST, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    SI_CUDA(cudaFuncSetAttribute(k_small_step<ST_WIDE, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
     SI_CUDA(cudaFuncSetAttribute(k_small_step<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
     SI_CUDA(cudaFuncSetAttribute(k_small_step<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1073,11 +1205,18 @@ void small_step_dev(const Exec& ex, LobpcgCtrl* ctrl, const double* gram, int ns
   }
   // the Rayleigh-Ritz problem has up to ns * m rows: up to 16 fit one warp's
   // registers; wider blocks get a CTA, the widest the most threads
-  if (ns * m > 24)
-    k_small_step<ST_WIDE><<<1, ST_WIDE, smem, ex.stream>>>(ctrl, gram, ns, mode);
-  else if (ns * m > WRR || small_step_variant() == 1)
-    k_small_step<ST><<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
-  else if (small_step_variant() == 2)
+  // (SPECTRAL_INIT_SMALL_STEP: unset, the CTA with the parallel Rayleigh-Ritz;
+  // serial, the CTA with one-thread-per-column triangular solves; warp / reg,
+  // one warp)
+  const int variant = small_step_variant();
+  const bool par = variant != 3;
+  if (ns * m > 24) {
+    if (par) k_small_step<ST_WIDE, false, true><<<1, ST_WIDE, smem, ex.stream>>>(ctrl, gram, ns, mode);
+    else k_small_step<ST_WIDE><<<1, ST_WIDE, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  } else if (ns * m > WRR || variant == 1 || variant == 3) {
+    if (par) k_small_step<ST, false, true><<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
+    else k_small_step<ST><<<1, ST, smem, ex.stream>>>(ctrl, gram, ns, mode);
+  } else if (variant == 2)
     k_small_step<32, true><<<1, 32, smem, ex.stream>>>(ctrl, gram, ns, mode);
   else
     k_small_step<32><<<1, 32, smem, ex.stream>>>(ctrl, gram, ns, mode);

@@ -288,13 +288,14 @@ def test_lobpcg_wide_blocks(gpu_ctx, nc, block, precision):
 
 
 @pytest.mark.parametrize("variant", ["task", "tile"])
-@pytest.mark.parametrize("small", ["warp", "cta", "reg"])
+@pytest.mark.parametrize("small", ["warp", "cta", "serial", "reg"])
 def test_lobpcg_kernel_variants_agree(gpu_ctx, monkeypatch, variant, small):
     """The 4-column LOBPCG iteration with either Gram kernel (task-split warps,
     default; register-tiled, SPECTRAL_INIT_GRAM=tile) and each small step (one
     warp with the Gram in shared memory, SPECTRAL_INIT_SMALL_STEP=warp; one
-    128-thread CTA, the default; one warp in registers, =reg) converges to the
-    dense eigenpairs."""
+    128-thread CTA with the parallel Rayleigh-Ritz, the default; the same CTA
+    with one-thread-per-column triangular solves, =serial; one warp in
+    registers, =reg) converges to the dense eigenpairs."""
     import spectral_init_b200 as si
     if variant == "tile":
         monkeypatch.setenv("SPECTRAL_INIT_GRAM", "tile")
