@@ -778,125 +778,6 @@ __device__ bool warp_rr_general(const double* gb, const double* ga, int P, const
   return true;
 }
 
-// Rotation of index x in round r of the round-robin pairing of cta_jacobi_db
-// (M = s2 - 1 odd: round r pairs r with M and every other x with
-// (2 r - x) mod M): its partner q and the coefficients of its new row and
-// column, new_x = al * x + be * q.  The angle is computed exactly as in
-// cta_jacobi_db, from the same matrix, so every thread that needs a pair's
-// rotation gets the same bits.
-__device__ __forceinline__ void jac_rotation(const double* cur, int ld, int x, int r, int M, int s, int& q,
-                                             double& al, double& be) {
-  int p;
-  if (x == M) {
-    p = r;
-  } else if (x == r) {
-    p = M;
-  } else {
-    p = 2 * r - x;
-    if (p < 0) p += M;
-    else if (p >= M) p -= M;
-  }
-  const int a = x < p ? x : p, b = x < p ? p : x;
-  double c = 1.0, sn = 0.0;
-  if (b < s) {
-    const double apq = cur[a * ld + b];
-    const double app = cur[a * ld + a], aqq = cur[b * ld + b];
-    const double tiny = DBL_EPSILON * 1e-3;
-    if (fabs(apq) > 1e-300 && apq * apq > tiny * tiny * fabs(app * aqq)) {
-      const float d = static_cast<float>(aqq - app), h = static_cast<float>(2.0 * apq);
-      const float tf = (d >= 0.0f ? h : -h) / (fabsf(d) + sqrtf(fmaf(d, d, h * h)));
-      const float cf = rsqrtf(fmaf(tf, tf, 1.0f));
-      c = static_cast<double>(cf);
-      sn = static_cast<double>(tf) * static_cast<double>(cf);
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const double f = fma(-0.5, fma(c, c, sn * sn), 1.5);
-        c *= f;
-        sn *= f;
-      }
-    }
-  }
-  // new row/column a = c a - s b ; new b = s a + c b
-  al = c;
-  if (x == a) {
-    be = -sn;
-    q = (b < s) ? b : a;
-  } else {
-    be = sn;
-    q = a;
-  }
-}
-
-// cta_jacobi_db with one barrier per round: instead of a few threads writing
-// the round's rotations to shared memory for the rest, every thread computes
-// the rotations of the rows and columns of its own update items.  Pays when a
-// thread has few items (2 s^2 <= 3 threads: the 12 x 12 problem of 4-column
-// blocks on 128 threads); bit-identical to cta_jacobi_db.
-__device__ void cta_jacobi_fused(double* A, double* V, double* A2, double* V2, int s, int ld, double* red) {
-  constexpr int kItems = 3;
-  const int s2 = s + (s & 1);
-  const int M = s2 - 1;
-  const int nitems = 2 * s * s;
-  int it_i[kItems], it_j[kItems];
-#pragma unroll
-  for (int q = 0; q < kItems; ++q) {
-    const int t = threadIdx.x + q * blockDim.x;
-    const int u = t < s * s ? t : t - s * s;
-    it_i[q] = u / s;
-    it_j[q] = u - (u / s) * s;
-  }
-  double* cur = A;
-  double* nxt = A2;
-  double* vc = V;
-  double* vn = V2;
-  for (int sweep = 0; sweep < 40; ++sweep) {
-    double off = 0.0, dia = 0.0;
-    for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
-      const int i = t / s, j = t - (t / s) * s;
-      const double a = cur[i * ld + j];
-      if (i == j) dia += a * a; else off += a * a;
-    }
-    off = cta_sum(off, red);
-    dia = cta_sum(dia, red);
-    if (!(off > jacobi_stop2(s) * dia)) break;
-    for (int r = 0; r < M; ++r) {
-#pragma unroll
-      for (int q = 0; q < kItems; ++q) {
-        const int t = threadIdx.x + q * blockDim.x;
-        if (t >= nitems) continue;
-        const int i = it_i[q], j = it_j[q];
-        int qj;
-        double alj, bej;
-        jac_rotation(cur, ld, j, r, M, s, qj, alj, bej);
-        if (t < s * s) {
-          int qi;
-          double ali, bei;
-          jac_rotation(cur, ld, i, r, M, s, qi, ali, bei);
-          nxt[i * ld + j] = ali * (alj * cur[i * ld + j] + bej * cur[i * ld + qj]) +
-                            bei * (alj * cur[qi * ld + j] + bej * cur[qi * ld + qj]);
-        } else {
-          vn[i * ld + j] = alj * vc[i * ld + j] + bej * vc[i * ld + qj];
-        }
-      }
-      __syncthreads();
-      double* tmp = cur;
-      cur = nxt;
-      nxt = tmp;
-      tmp = vc;
-      vc = vn;
-      vn = tmp;
-    }
-  }
-  if (cur != A) {
-    for (int t = threadIdx.x; t < s * s; t += blockDim.x) {
-      const int i = t / s, j = t - (t / s) * s;
-      A[i * ld + j] = cur[i * ld + j];
-      V[i * ld + j] = vc[i * ld + j];
-    }
-  }
-  __syncthreads();
-}
-
 // The generalised Rayleigh-Ritz of cta_rr_general with its serial sections
 // made parallel: the D-scale factors one per thread; a right-looking
 // Cholesky with one barrier per pivot (every thread recomputes the pivot, the
@@ -904,9 +785,7 @@ __device__ void cta_jacobi_fused(double* A, double* V, double* A2, double* V2, i
 // one pass at the end); L^-1 formed once, one column per thread, so that
 // C = L^-1 A L^-T and the Ritz vectors D L^-T V_sel are parallel matrix
 // products instead of three one-thread-per-column triangular solves; the
-// selection order by ranks; the Jacobi rounds of small problems with one
-// barrier each (cta_jacobi_fused).  Same results as cta_rr_general up to
-// rounding.
+// selection order by ranks.  Same results as cta_rr_general up to rounding.
 __device__ bool cta_rr_general_par(const double* gb, const double* ga, int P, const int* idx, int s, int nsel,
                                    int largest, double chol_tol, SmallSmem sm, double* dsc, double* theta_out,
                                    double* red, int* order, int* sflag) {
@@ -995,8 +874,7 @@ __device__ bool cta_rr_general_par(const double* gb, const double* ga, int P, co
   __syncthreads();
   cta_identity(sm.V, s, ld);
   __syncthreads();
-  if (2 * s * s <= 3 * static_cast<int>(blockDim.x)) cta_jacobi_fused(sm.A, sm.V, sm.T, sm.Z, s, ld, red);
-  else cta_jacobi_db(sm.A, sm.V, sm.T, sm.Z, s, ld, red);
+  cta_jacobi_db(sm.A, sm.V, sm.T, sm.Z, s, ld, red);
   // ---- selection by ranks (ascending, or descending for `largest`; ties by index) ----
   for (int i = threadIdx.x; i < s; i += nt) {
     const double di = sm.A[i * ld + i];
