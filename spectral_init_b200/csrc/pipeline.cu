@@ -110,6 +110,119 @@ __global__ void k_centroid_sums(int64_t n, int nf, const float* __restrict__ dat
   }
 }
 
+// ---- meta-embedding on the device (src/multi_component.rs:143-255) -----------
+// Every kernel below sums in the order of the crate's loops (features, then
+// columns ascending), one thread per output, so the result does not depend on
+// the launch shape.
+
+// cent[c, :] /= size_c (the centroid means; empty components stay zero)
+__global__ void k_centroid_mean(int64_t ncomp, int nf, const uint64_t* __restrict__ comp_off,
+                                double* __restrict__ cent) {
+  const int64_t total = ncomp * nf;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total; e += stride) {
+    const int64_t c = e / nf;
+    const uint64_t sz = comp_off[c + 1] - comp_off[c];
+    if (sz != 0) cent[e] *= 1.0 / static_cast<double>(sz);
+  }
+}
+
+// aff[i, j] = exp(-||cent_i - cent_j||^2)
+__global__ void k_meta_affinity(int64_t ncomp, int nf, const double* __restrict__ cent, double* __restrict__ aff) {
+  const int64_t total = ncomp * ncomp;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total; e += stride) {
+    const int64_t i = e / ncomp, j = e % ncomp;
+    double d2 = 0.0;
+    for (int f = 0; f < nf; ++f) {
+      const double dd = cent[i * nf + f] - cent[j * nf + f];
+      d2 += dd * dd;
+    }
+    aff[e] = exp(-d2);
+  }
+}
+
+// degree of row i without the self affinity: inv_sqrt = d^-1/2 (0 for an
+// isolated centroid), sqrt_deg = d^1/2
+__global__ void k_meta_degrees(int64_t ncomp, const double* __restrict__ aff, double* __restrict__ inv_sqrt,
+                               double* __restrict__ sqrt_deg) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < ncomp; i += stride) {
+    double s = 0.0;
+    for (int64_t j = 0; j < ncomp; ++j)
+      if (j != i) s += aff[i * ncomp + j];
+    inv_sqrt[i] = s > 0.0 ? 1.0 / sqrt(s) : 0.0;
+    sqrt_deg[i] = sqrt(s);
+  }
+}
+
+// the normalised Laplacian I - D^-1/2 W D^-1/2 as a CSR with every entry of
+// each row stored (row i at [i * ncomp, (i + 1) * ncomp))
+__global__ void k_meta_laplacian(int64_t ncomp, const double* __restrict__ aff, const double* __restrict__ inv_sqrt,
+                                 uint64_t* __restrict__ indptr, uint32_t* __restrict__ indices,
+                                 double* __restrict__ values) {
+  const int64_t total = ncomp * ncomp;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e <= total; e += stride) {
+    if (e % ncomp == 0) indptr[e / ncomp] = static_cast<uint64_t>(e);
+    if (e == total) continue;
+    const int64_t i = e / ncomp, j = e % ncomp;
+    indices[e] = static_cast<uint32_t>(j);
+    values[e] = (i == j) ? 1.0 : -inv_sqrt[i] * aff[e] * inv_sqrt[j];
+  }
+}
+
+// meta[i, d] = vecs[i, sel[d]] (the selected eigenvectors, row-major [ncomp x k])
+__global__ void k_meta_gather(int64_t ncomp, int dims, const double* __restrict__ vecs, int k,
+                              const int* __restrict__ sel, double* __restrict__ meta) {
+  const int64_t total = ncomp * dims;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total; e += stride) {
+    const int64_t i = e / dims;
+    const int d = static_cast<int>(e % dims);
+    meta[e] = vecs[i * k + sel[d]];
+  }
+}
+
+// x /= d (the meta coordinates over their largest magnitude)
+__global__ void k_divide(int64_t count, double d, double* __restrict__ x) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < count; e += stride) x[e] /= d;
+}
+
+// the orthogonal layout (src/multi_component.rs:127-140): component c at
+// +e_(c mod dims) for the first dims components, -e_(c mod dims) after
+__global__ void k_meta_orthogonal(int64_t ncomp, int dims, double* __restrict__ meta) {
+  const int64_t total = ncomp * dims;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total; e += stride) {
+    const int64_t c = e / dims;
+    const int d = static_cast<int>(e % dims);
+    meta[e] = (d == c % dims) ? (c < dims ? 1.0 : -1.0) : 0.0;
+  }
+}
+
+// ranges[c] = half the distance to the nearest other (distinct) component
+// position, 1 when there is none (src/multi_component.rs:224-255)
+__global__ void k_meta_ranges(int64_t ncomp, int dims, const double* __restrict__ meta, double* __restrict__ ranges) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < ncomp; c += stride) {
+    double md = INFINITY;
+    for (int64_t i = 0; i < ncomp; ++i) {
+      if (i == c) continue;
+      double s = 0.0;
+      for (int d = 0; d < dims; ++d) {
+        const double df = meta[c * dims + d] - meta[i * dims + d];
+        s += df * df;
+      }
+      const double dist = sqrt(s);
+      if (dist > 0.0 && dist < md) md = dist;
+    }
+    ranges[c] = (ncomp > 1 && isfinite(md)) ? md / 2.0 : 1.0;
+  }
+}
+
+
 int grid_for(const Exec& ex, int64_t items) {
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((items + 255) / 256, int64_t(ex.sms) * 16)));
 }
@@ -227,9 +340,9 @@ void embed_disconnected_dev(const Exec& ex, const GraphDev& g, const uint32_t* l
   SI_CUDA(cudaMemcpyAsync(h_pptr.data(), pptr.get(), sizeof(uint64_t) * (n + 1), cudaMemcpyDeviceToHost, ex.stream));
   SI_CUDA(cudaStreamSynchronize(ex.stream));
 
-  // ---- meta-embedding (src/multi_component.rs:31-51, :127-220) ------------------
+  // ---- meta-embedding (src/multi_component.rs:31-51, :127-255), on the device ----
   const int dims = nc;
-  std::vector<double> meta(static_cast<size_t>(ncomp) * dims, 0.0);
+  DevBuf<double> dmeta_all(static_cast<size_t>(ncomp) * dims, ex.stream);
   if (ncomp > 2 * dims) {
     if (data_dev == nullptr)
       throw Error(SI_INVALID_GRAPH,
@@ -240,95 +353,51 @@ void embed_disconnected_dev(const Exec& ex, const GraphDev& g, const uint32_t* l
     cent.zero();
     k_centroid_sums<<<grid_for(ex, n * nf), 256, 0, ex.stream>>>(n, nf, data_dev, labels, cent.get());
     SI_LAUNCH_CHECK();
-    std::vector<double> hc(static_cast<size_t>(ncomp) * nf);
-    SI_CUDA(cudaMemcpyAsync(hc.data(), cent.get(), sizeof(double) * hc.size(), cudaMemcpyDeviceToHost, ex.stream));
-    SI_CUDA(cudaStreamSynchronize(ex.stream));
-    for (int64_t c = 0; c < ncomp; ++c) {
-      const double sz = static_cast<double>(h_off[c + 1] - h_off[c]);
-      if (sz == 0.0) continue;
-      const double inv_size = 1.0 / sz;
-      for (int f = 0; f < nf; ++f) hc[c * nf + f] *= inv_size;
-    }
+    k_centroid_mean<<<grid_for(ex, ncomp * nf), 256, 0, ex.stream>>>(ncomp, nf, coff.get(), cent.get());
+    SI_LAUNCH_CHECK();
     // Gaussian affinity and the normalised Laplacian of the centroid graph
-    std::vector<double> aff(static_cast<size_t>(ncomp) * ncomp);
-    for (int64_t i = 0; i < ncomp; ++i)
-      for (int64_t j = 0; j < ncomp; ++j) {
-        double d2 = 0.0;
-        for (int f = 0; f < nf; ++f) {
-          const double dd = hc[i * nf + f] - hc[j * nf + f];
-          d2 += dd * dd;
-        }
-        aff[i * ncomp + j] = std::exp(-d2);
-      }
-    std::vector<double> degm(ncomp), invm(ncomp), sqm(ncomp);
-    for (int64_t i = 0; i < ncomp; ++i) {
-      double s = 0.0;
-      for (int64_t j = 0; j < ncomp; ++j)
-        if (j != i) s += aff[i * ncomp + j];
-      degm[i] = s;
-      invm[i] = s > 0.0 ? 1.0 / std::sqrt(s) : 0.0;
-      sqm[i] = std::sqrt(s);
-    }
-    std::vector<uint64_t> lp(ncomp + 1);
-    std::vector<uint32_t> li;
-    std::vector<double> lv;
-    for (int64_t i = 0; i < ncomp; ++i) {
-      lp[i] = li.size();
-      for (int64_t j = 0; j < ncomp; ++j) {
-        const double v = (i == j) ? 1.0 : -invm[i] * aff[i * ncomp + j] * invm[j];
-        if (i == j || v != 0.0) {
-          li.push_back(static_cast<uint32_t>(j));
-          lv.push_back(v);
-        }
-      }
-    }
-    lp[ncomp] = li.size();
+    const int64_t mnnz = ncomp * ncomp;
+    DevBuf<double> aff(static_cast<size_t>(mnnz), ex.stream), invm(ncomp, ex.stream), dsq(ncomp, ex.stream);
+    k_meta_affinity<<<grid_for(ex, mnnz), 256, 0, ex.stream>>>(ncomp, nf, cent.get(), aff.get());
+    SI_LAUNCH_CHECK();
+    k_meta_degrees<<<grid_for(ex, ncomp), 256, 0, ex.stream>>>(ncomp, aff.get(), invm.get(), dsq.get());
+    SI_LAUNCH_CHECK();
     DevBuf<uint64_t> dlp(ncomp + 1, ex.stream);
-    DevBuf<uint32_t> dli(li.size(), ex.stream);
-    DevBuf<double> dlv(lv.size(), ex.stream), dsq(ncomp, ex.stream);
-    SI_CUDA(cudaMemcpyAsync(dlp.get(), lp.data(), sizeof(uint64_t) * lp.size(), cudaMemcpyHostToDevice, ex.stream));
-    SI_CUDA(cudaMemcpyAsync(dli.get(), li.data(), sizeof(uint32_t) * li.size(), cudaMemcpyHostToDevice, ex.stream));
-    SI_CUDA(cudaMemcpyAsync(dlv.get(), lv.data(), sizeof(double) * lv.size(), cudaMemcpyHostToDevice, ex.stream));
-    SI_CUDA(cudaMemcpyAsync(dsq.get(), sqm.data(), sizeof(double) * sqm.size(), cudaMemcpyHostToDevice, ex.stream));
-    OpDev mop = op_from_csr64(dlp.get(), dli.get(), dlv.get(), ncomp, static_cast<int64_t>(li.size()));
+    DevBuf<uint32_t> dli(static_cast<size_t>(mnnz), ex.stream);
+    DevBuf<double> dlv(static_cast<size_t>(mnnz), ex.stream);
+    k_meta_laplacian<<<grid_for(ex, mnnz + 1), 256, 0, ex.stream>>>(ncomp, aff.get(), invm.get(), dlp.get(), dli.get(),
+                                                                   dlv.get());
+    SI_LAUNCH_CHECK();
+    OpDev mop = op_from_csr64(dlp.get(), dli.get(), dlv.get(), ncomp, mnnz);
     EigenResult r;
     SolverStats mst;
     SolverConfig msc = pc.solver;
     msc.precision = SI_PRECISION_FP64;
     msc.force_level = -1;
     solve_eigenproblem_dev(ex, mop, dims, seed, dsq.get(), msc, r, mst);
-    const std::vector<int> order = selection_order(r.vals, dims);
-    std::vector<double> hv(static_cast<size_t>(ncomp) * r.k);
-    SI_CUDA(cudaMemcpyAsync(hv.data(), r.vecs.get(), sizeof(double) * hv.size(), cudaMemcpyDeviceToHost, ex.stream));
-    SI_CUDA(cudaStreamSynchronize(ex.stream));
-    double mx = 0.0;
-    for (int64_t i = 0; i < ncomp; ++i)
-      for (int d = 0; d < dims; ++d) {
-        meta[i * dims + d] = hv[i * r.k + order[d]];
-        mx = std::max(mx, std::fabs(meta[i * dims + d]));
-      }
+    const std::vector<int> sel = selection_order(r.vals, dims);
+    DevBuf<int> dsel(dims, ex.stream);
+    SI_CUDA(cudaMemcpyAsync(dsel.get(), sel.data(), sizeof(int) * dims, cudaMemcpyHostToDevice, ex.stream));
+    k_meta_gather<<<grid_for(ex, ncomp * dims), 256, 0, ex.stream>>>(ncomp, dims, r.vecs.get(), r.k, dsel.get(),
+                                                                     dmeta_all.get());
+    SI_LAUNCH_CHECK();
+    GramWork gwm;
+    const double mx = max_abs_dev(ex, gwm, dmeta_all.get(), ncomp, dims, dims);
     if (mx == 0.0) throw Error(SI_INVALID_GRAPH, "invalid graph: spectral meta-embedding produced all-zero result");
-    for (double& v : meta) v /= mx;
+    k_divide<<<grid_for(ex, ncomp * dims), 256, 0, ex.stream>>>(ncomp * dims, mx, dmeta_all.get());
+    SI_LAUNCH_CHECK();
   } else {
-    for (int64_t row = 0; row < ncomp; ++row) meta[row * dims + row % dims] = row < dims ? 1.0 : -1.0;
+    k_meta_orthogonal<<<grid_for(ex, ncomp * dims), 256, 0, ex.stream>>>(ncomp, dims, dmeta_all.get());
+    SI_LAUNCH_CHECK();
   }
-  // data ranges (src/multi_component.rs:224-255)
+  // data ranges (src/multi_component.rs:224-255); the host needs them for the scale factors
   std::vector<double> ranges(ncomp, 1.0);
-  if (ncomp > 1) {
-    for (int64_t c = 0; c < ncomp; ++c) {
-      double md = INFINITY;
-      for (int64_t i = 0; i < ncomp; ++i) {
-        if (i == c) continue;
-        double s = 0.0;
-        for (int d = 0; d < dims; ++d) {
-          const double df = meta[c * dims + d] - meta[i * dims + d];
-          s += df * df;
-        }
-        const double dist = std::sqrt(s);
-        if (dist > 0.0 && dist < md) md = dist;
-      }
-      ranges[c] = std::isfinite(md) ? md / 2.0 : 1.0;
-    }
+  {
+    DevBuf<double> dranges(ncomp, ex.stream);
+    k_meta_ranges<<<grid_for(ex, ncomp), 256, 0, ex.stream>>>(ncomp, dims, dmeta_all.get(), dranges.get());
+    SI_LAUNCH_CHECK();
+    SI_CUDA(cudaMemcpyAsync(ranges.data(), dranges.get(), sizeof(double) * ncomp, cudaMemcpyDeviceToHost, ex.stream));
+    SI_CUDA(cudaStreamSynchronize(ex.stream));
   }
   // ---- per component (src/multi_component.rs:261-312) -----------------------------
   // Components are independent: worker threads, each with its own stream,
@@ -346,13 +415,12 @@ void embed_disconnected_dev(const Exec& ex, const GraphDev& g, const uint32_t* l
   std::atomic<bool> failed{false};
   std::mutex mu;
   std::exception_ptr first_error;
-  auto solve_one = [&](const Exec& wex, GramWork& gw, DevBuf<double>& dmeta, int64_t c) {
+  auto solve_one = [&](const Exec& wex, GramWork& gw, int64_t c) {
     const int64_t off = static_cast<int64_t>(h_off[c]);
     const int64_t sz = static_cast<int64_t>(h_off[c + 1] - h_off[c]);
-    SI_CUDA(cudaMemcpyAsync(dmeta.get(), meta.data() + c * dims, sizeof(double) * dims, cudaMemcpyHostToDevice,
-                            wex.stream));
+    const double* dmeta = dmeta_all.get() + c * dims;  // written on ex.stream, synchronised above
     if (sz < 2 * dims) {
-      k_place<<<grid_for(wex, sz * dims), 256, 0, wex.stream>>>(sz, off, perm.get(), nullptr, dims, 0.0, dmeta.get(),
+      k_place<<<grid_for(wex, sz * dims), 256, 0, wex.stream>>>(sz, off, perm.get(), nullptr, dims, 0.0, dmeta,
                                                                  result.get());
       SI_LAUNCH_CHECK();
       SI_CUDA(cudaStreamSynchronize(wex.stream));
@@ -376,7 +444,7 @@ void embed_disconnected_dev(const Exec& ex, const GraphDev& g, const uint32_t* l
     embed_connected(wex, sub, dims, seed, pc, coords, cst, ev);
     const double mx = max_abs_dev(wex, gw, coords.get(), sz, dims, dims);
     const double s = mx > 0.0 ? ranges[c] / mx : 1.0;
-    k_place<<<grid_for(wex, sz * dims), 256, 0, wex.stream>>>(sz, off, perm.get(), coords.get(), dims, s, dmeta.get(),
+    k_place<<<grid_for(wex, sz * dims), 256, 0, wex.stream>>>(sz, off, perm.get(), coords.get(), dims, s, dmeta,
                                                                result.get());
     SI_LAUNCH_CHECK();
     SI_CUDA(cudaStreamSynchronize(wex.stream));
@@ -394,11 +462,10 @@ void embed_disconnected_dev(const Exec& ex, const GraphDev& g, const uint32_t* l
       Exec wex = ex;
       wex.stream = st;
       GramWork gw;
-      DevBuf<double> dmeta(dims, st);
       for (;;) {
         const int64_t i = next.fetch_add(1);
         if (i >= ncomp || failed.load()) break;
-        solve_one(wex, gw, dmeta, order[i]);
+        solve_one(wex, gw, order[i]);
       }
     } catch (...) {
       std::lock_guard<std::mutex> lk(mu);
