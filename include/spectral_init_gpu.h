@@ -178,6 +178,19 @@ si_status si_build_laplacian_csr(si_ctx* ctx, const si_csr_f32* graph, const dou
                                  uint64_t* out_indptr, uint32_t* out_indices, double* out_data,
                                  uint64_t* out_nnz);
 
+/* The fuzzy-kNN graph the crate consumes, built from points the way its
+ * fixture generator builds it (tests/generate_fixtures.py:70-182): exact
+ * Euclidean kNN without the point itself (knn_indices i32 / knn_dists f32
+ * [n x k]), umap-learn's smooth-kNN sigmas / rhos (f32 [n]), membership
+ * strengths, the fuzzy union A + A^T - A.A^T and pruning below
+ * max / n_epochs.  points: f64 [n x dims] row-major; the pruned graph goes to
+ * indptr (u64 [n + 1]) / indices (u32) / data (f32) with room for `capacity`
+ * entries (2 n k always suffices), its entry count to *nnz.  All device
+ * pointers; k <= 32, dims <= 256; brute force (O(n^2 dims)). */
+si_status si_fuzzy_graph(si_ctx* ctx, const double* points, uint64_t n, uint32_t dims, uint32_t k,
+                         int32_t* knn_indices, float* knn_dists, float* sigmas, float* rhos, uint64_t* indptr,
+                         uint32_t* indices, float* data, uint64_t capacity, uint64_t* nnz);
+
 /* find_components (src/components.rs:7-44): labels numbered by the smallest
  * node of each component (BFS start order).  labels: device u32 [n]. */
 si_status si_find_components(si_ctx* ctx, const si_csr_f32* graph, uint32_t* labels,

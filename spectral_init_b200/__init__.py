@@ -5,6 +5,7 @@ The numerical work lives in ``libspectral_init_b200.so`` (C ABI declared in
 crate's public API.
 """
 from .api import (  # noqa: F401
+    fuzzy_graph,
     ComputeMode,
     Context,
     ConvergenceFailure,

@@ -78,6 +78,8 @@ _SIGNATURES = {
     "si_build_laplacian": (C.c_int, [vp, C.POINTER(SiCsrF32), vp, vp, vp]),
     "si_build_laplacian_csr": (C.c_int, [vp, C.POINTER(SiCsrF32), vp, vp, vp, vp, u64p]),
     "si_find_components": (C.c_int, [vp, C.POINTER(SiCsrF32), vp, u64p]),
+    "si_fuzzy_graph": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32, C.c_uint32, vp, vp, vp, vp, vp, vp, vp,
+                                 C.c_uint64, u64p]),
     "si_spmm": (C.c_int, [vp, C.POINTER(SiOperator), vp, vp, C.c_uint32]),
     "si_spmm_f32": (C.c_int, [vp, C.POINTER(SiOperator), vp, vp, C.c_uint32]),
     "si_operator_plan_create": (C.c_int, [vp, C.POINTER(SiOperator), C.POINTER(vp)]),

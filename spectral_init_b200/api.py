@@ -316,6 +316,38 @@ def build_normalized_laplacian(graph, inv_sqrt_deg, *, ctx: Context | None = Non
                           ip.cpu().numpy()), shape=(g.n, g.n))
 
 
+def fuzzy_graph(points, k: int = 15, *, ctx: Context | None = None, return_stages: bool = False):
+    """The fuzzy-kNN graph of ``points`` ([n, dims]) on the device, as the
+    crate's fixture generator builds it (tests/generate_fixtures.py:70-182):
+    exact kNN without the point itself, umap-learn's smooth-kNN, membership
+    strengths, fuzzy union, pruning.  Returns the scipy CSR (f32), and with
+    ``return_stages`` also (knn_indices, knn_dists, sigmas, rhos)."""
+    import scipy.sparse as sp
+    ctx = ctx or get_context()
+    torch = _torch()
+    dev = f"cuda:{ctx.device}"
+    x = torch.as_tensor(np.ascontiguousarray(points, dtype=np.float64), device=dev)
+    n, d = x.shape
+    cap = 2 * n * k
+    idx = torch.empty(n, k, dtype=torch.int32, device=dev)
+    dist = torch.empty(n, k, dtype=torch.float32, device=dev)
+    sig = torch.empty(n, dtype=torch.float32, device=dev)
+    rho = torch.empty(n, dtype=torch.float32, device=dev)
+    ip = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    ix = torch.empty(max(cap, 1), dtype=torch.int32, device=dev)
+    dv = torch.empty(max(cap, 1), dtype=torch.float32, device=dev)
+    nnz = C.c_uint64(0)
+    torch.cuda.synchronize()
+    ctx.check(ctx.lib.si_fuzzy_graph(ctx.ptr, x.data_ptr(), n, d, k, idx.data_ptr(), dist.data_ptr(), sig.data_ptr(),
+                                     rho.data_ptr(), ip.data_ptr(), ix.data_ptr(), dv.data_ptr(), cap,
+                                     C.byref(nnz)))
+    m = int(nnz.value)
+    g = sp.csr_matrix((dv[:m].cpu().numpy(), ix[:m].cpu().numpy(), ip.cpu().numpy()), shape=(n, n))
+    if return_stages:
+        return g, (idx.cpu().numpy(), dist.cpu().numpy(), sig.cpu().numpy(), rho.cpu().numpy())
+    return g
+
+
 def find_components(graph, *, ctx: Context | None = None):
     """find_components (src/components.rs:7-44) -> (labels, n_components)."""
     ctx = ctx or get_context()

@@ -383,6 +383,17 @@ si_status si_build_laplacian_csr(si_ctx* ctx, const si_csr_f32* graph, const dou
   });
 }
 
+si_status si_fuzzy_graph(si_ctx* ctx, const double* points, uint64_t n, uint32_t dims, uint32_t k,
+                         int32_t* knn_indices, float* knn_dists, float* sigmas, float* rhos, uint64_t* indptr,
+                         uint32_t* indices, float* data, uint64_t capacity, uint64_t* nnz) {
+  return guarded(ctx, [&] {
+    SI_REQUIRE(points && knn_indices && knn_dists && sigmas && rhos && indptr && indices && data && nnz,
+               SI_INVALID_ARGUMENT, "fuzzy graph: null pointer");
+    si::fuzzy_graph_dev(ctx->ex(), points, static_cast<int64_t>(n), static_cast<int>(dims), static_cast<int>(k),
+                        knn_indices, knn_dists, sigmas, rhos, indptr, indices, data, capacity, nnz);
+  });
+}
+
 si_status si_find_components(si_ctx* ctx, const si_csr_f32* graph, uint32_t* labels, uint64_t* n_components) {
   return guarded(ctx, [&] {
     const si::Exec ex = ctx->ex();

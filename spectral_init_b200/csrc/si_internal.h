@@ -139,6 +139,13 @@ OpDev op_from_csr64(const uint64_t* indptr, const uint32_t* indices, const doubl
 // Exclusive scan of u64 counts (device), returns the total.
 uint64_t exclusive_scan_u64(const Exec& ex, const uint64_t* in, uint64_t* out, int64_t n);
 
+// ---- fuzzy.cu --------------------------------------------------------------------
+// The fuzzy-kNN graph from f64 points [n x d] (exact kNN, smooth-kNN,
+// memberships, fuzzy union, pruning); see si_fuzzy_graph.
+void fuzzy_graph_dev(const Exec& ex, const double* x, int64_t n, int d, int k, int32_t* knn_idx, float* knn_dist,
+                     float* sigma, float* rho, uint64_t* indptr, uint32_t* indices, float* data, uint64_t capacity,
+                     uint64_t* nnz_out);
+
 // ---- components.cu --------------------------------------------------------
 int64_t find_components_dev(const Exec& ex, const GraphDev& g, uint32_t* labels);
 

@@ -1,0 +1,51 @@
+"""The device fuzzy-kNN construction (si_fuzzy_graph, csrc/fuzzy.cu) against
+the reference's stage fixtures (tests/generate_fixtures.py:70-182) and the
+oracle (oracle/fuzzy_oracle.py): exact kNN, smooth-kNN sigma / rho, and the
+pruned fuzzy union, on the datasets whose stage inputs are committed."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import GOLDEN
+from oracle import fuzzy_oracle as F
+
+pytestmark = pytest.mark.gpu
+
+
+def _npz(ds, name):
+    return np.load(GOLDEN / ds / f"{name}.npz", allow_pickle=False)
+
+
+@pytest.mark.parametrize("ds", ["blobs_connected_200", "moons_200", "near_dupes_100"])
+def test_fuzzy_graph_stages_match_fixtures(gpu_ctx, ds):
+    import spectral_init_b200 as si
+    x = _npz(ds, "step0_raw_data")["X"]
+    ref1 = _npz(ds, "step1_knn_exact")
+    ref2 = _npz(ds, "step2_smooth_knn_exact")
+    k = int(ref1["n_neighbors"])
+    g, (idx, dist, sig, rho) = si.fuzzy_graph(x, k, ctx=gpu_ctx, return_stages=True)
+    assert np.allclose(dist, ref1["knn_dists"], rtol=1e-6, atol=1e-7)
+    assert np.allclose(rho, ref2["rhos"], rtol=1e-6, atol=1e-7)
+    assert np.allclose(sig, ref2["sigmas"], rtol=1e-5, atol=1e-7)  # +inf rows included
+    if ds == "near_dupes_100":
+        return  # duplicated points tie: which duplicate is a neighbour is not pinned
+    assert np.array_equal(idx, ref1["knn_indices"])
+    ref5 = sp.load_npz(GOLDEN / ds / "step5a_pruned_exact.npz").tocsr()
+    ref5.sort_indices()
+    assert np.array_equal(g.indptr, ref5.indptr) and np.array_equal(g.indices, ref5.indices)
+    assert np.allclose(g.data, ref5.data, rtol=2e-6, atol=1e-7)
+
+
+def test_fuzzy_graph_matches_oracle_on_a_larger_cloud(gpu_ctx):
+    """3000 points of a 6-cluster mixture in 10-D, k = 15: the device graph
+    equals the oracle's (structure exactly, values to f32 rounding)."""
+    import spectral_init_b200 as si
+    rng = np.random.default_rng(5)
+    centres = rng.normal(0, 4, (6, 10))
+    x = np.concatenate([rng.normal(0, 1, (500, 10)) + c for c in centres])
+    g = si.fuzzy_graph(x, 15, ctx=gpu_ctx)
+    ref = F.fuzzy_graph(x, 15)
+    ref.sort_indices()
+    assert np.array_equal(g.indptr, ref.indptr) and np.array_equal(g.indices, ref.indices)
+    assert np.allclose(g.data, ref.data, rtol=2e-6, atol=1e-7)
+    assert (g != g.T).nnz == 0
